@@ -1,0 +1,286 @@
+"""Benchmark: sieved primes/s of the B200 siever on the plain full-size item.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c2|c3|c1] [--width W] [--plain]
+
+One step is one pass of the hot path (segment sieve -> prep -> exact BSGS ->
+order) over one item's whole P range, through the C-ABI (mps_item_relations).
+Default workload (the plain GPU path, full size): b=10, c=111,
+10^12 <= p < 10^12 + 10^10, 0 <= n < 10^7, n == 4 (mod 6).
+
+Under torchrun (N > 1) every rank sieves its own P slice of the same width
+(weak scaling, no data-path collective); the per-step time is the max over
+ranks.  Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "mass-prime-siever_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+WORKLOADS = {
+    # name: (b, c, P0, width, N0, N1, mod, res, label)
+    "c2": (10, 111, 10**12, 10**10, 0, 10**7, 6, 4,
+           "plain GPU path, full size: b=10 c=111 p in [1e12, 1e12+1e10) n in [0, 1e7) n==4 mod 6"),
+    "c3": (2, -25, 95 * 10**12, 2 * 10**10, 3_600_000, 5_000_000, 2, 1,
+           "residue classes: b=2 c=-25 p in [9.5e13, 9.5e13+2e10) n in [3.6e6, 5e6) n==1 mod 2"),
+    "c1": (2, -25, 10**6, 10**8 - 10**6, 0, 100_000, 2, 1,
+           "small CPU-runnable: b=2 c=-25 p in [1e6, 1e8) n in [0, 1e5) n==1 mod 2"),
+}
+CPU_SAMPLE_WIDTH = {"c2": 30_000_000, "c3": 20_000_000, "c1": 99_000_000}
+
+
+def peaks_file():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+class ClockSampler:
+    """nvidia-smi samples (SM clock, throttle reasons) during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.reader.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        return rank, world, local, dist
+    return 0, 1, 0, None
+
+
+def max_over_ranks(dist, local: int, value: float) -> float:
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(dist, local: int, value: float) -> float:
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(dist, local: int):
+    if dist is not None:
+        import torch
+        dist.barrier(device_ids=[local])
+        torch.cuda.synchronize(local)
+
+
+def cpu_reference_rate(spec, width: int, threads: int):
+    """The reference's own segmented_sieve + run_bsgs (oracle/_ref, threaded like
+    run_worker_pool) on [P0, P0 + width): (primes/s, primes, seconds, kind)."""
+    from oracle.oracle import Oracle, Reference, make_item as oracle_item
+    b, c, P0, _, N0, N1, mod, res, _ = spec
+    it = oracle_item(b, c, P0, P0 + width, N0, N1, mod, res)
+    if Reference.available():
+        ref = Reference()
+        t0 = time.perf_counter()
+        rels, nprimes = ref.relations(P0, P0 + width, it, threads=threads)
+        dt = time.perf_counter() - t0
+        return nprimes / dt, nprimes, dt, "reference", len(rels)
+    orc = Oracle()
+    t0 = time.perf_counter()
+    rels = orc.relations(P0, P0 + width, it, threads=threads)
+    dt = time.perf_counter() - t0
+    nprimes = len(orc.primes(P0, P0 + width, 1 << 22))
+    return nprimes / dt, nprimes, dt, "port", len(rels)
+
+
+def run_reference(args, spec, label):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    width = CPU_SAMPLE_WIDTH[args.workload] if args.width is None else min(int(args.width), CPU_SAMPLE_WIDTH[args.workload])
+    for _ in range(args.warmup):
+        cpu_reference_rate(spec, max(width // 10, 1_000_000), threads)
+    rates, primes_total, secs = [], 0, 0.0
+    kind = "reference"
+    for _ in range(args.steps):
+        rate, nprimes, dt, kind, _ = cpu_reference_rate(spec, width, threads)
+        rates.append(rate)
+        primes_total += nprimes
+        secs += dt
+    value = primes_total / secs
+    sample = f"[P0, P0+{width:.3g}) of the workload per step, {threads} threads"
+    line = {
+        "impl": "reference", "metric": "sieved primes/s", "value": value, "unit": "primes/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": label, "P_width_per_step": width},
+        "cpu_baseline": {"value": value, "unit": "primes/s", "cores": threads, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": "primes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--width", type=float, default=None, help="P width per rank (default: the workload's)")
+    ap.add_argument("--plain", action="store_true", help="the plain per-chunk path")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    spec = WORKLOADS[args.workload]
+    b, c, P0, width, N0, N1, mod, res, label = spec
+    if args.width is not None:
+        width = int(args.width)
+
+    if args.impl == "reference":
+        return run_reference(args, spec, label)
+
+    rank, world, local, dist = dist_setup(args.gpus)
+    import mps_b200
+    lo = P0 + rank * width
+    hi = lo + width
+    item = mps_b200.make_item(b, c, lo, hi, N0, N1, mod, res)
+    siever = mps_b200.Siever(local, plain=1 if args.plain else 0)
+
+    # units: primes in this rank's slice (counted on the device, outside the timed region)
+    nprimes = siever.count_primes(lo, hi)
+    total_primes = sum_over_ranks(dist, local, float(nprimes))
+
+    for _ in range(args.warmup):
+        siever.item_relations(item)
+
+    clocks = ClockSampler(local)
+    barrier(dist, local)
+    clocks.start()
+    t0 = time.perf_counter()
+    dev_ms, bsgs_ms, steps_done, launches, rel_count, entries = 0.0, 0.0, 0, 0, 0, 0
+    for _ in range(args.steps):
+        rels = siever.item_relations(item)
+        st = siever.stats()
+        dev_ms += st["device_ms"]
+        bsgs_ms += st["bsgs_ms"]
+        steps_done += st["bsgs_steps"]
+        launches += st["kernel_launches"]
+        rel_count = len(rels)
+        entries = st["entries"]
+    wall = time.perf_counter() - t0
+    barrier(dist, local)
+    clk = clocks.stop()
+
+    dev_s = max_over_ranks(dist, local, dev_ms / 1e3)
+    wall_s = max_over_ranks(dist, local, wall)
+    value = total_primes * args.steps / dev_s
+    e2e = total_primes * args.steps / wall_s
+
+    mmul_peak, imad_peak = siever.measure_peaks()
+    bsgs_rate = steps_done / (bsgs_ms / 1e3) if bsgs_ms > 0 else 0.0
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        cw = CPU_SAMPLE_WIDTH[args.workload]
+        rate, np_, dt, kind, _ = cpu_reference_rate(spec, cw, threads)
+        cpu = {"value": rate, "unit": "primes/s", "cores": threads, "kind": kind,
+               "sample": f"[{P0:.4g}, {P0:.4g}+{cw:.3g}) of the same item ({np_} primes, {dt:.1f} s)"}
+
+    if rank == 0:
+        line = {
+            "metric": "sieved primes/s", "value": value, "unit": "primes/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic",
+            "config": {"workload": label, "P_width_per_gpu": width, "path": "plain" if args.plain else "persistent",
+                       "l2": "working set (survivors, entries) > 126 MB L2 per chunk; no flush"},
+            "e2e": {"value": e2e, "unit": "primes/s", "h2d_bytes_per_step": 112,
+                    "d2h_bytes_per_step": 24 * rel_count},
+            "gpu_launches": launches,
+            "relations": rel_count, "bsgs_primes": entries, "primes": int(total_primes),
+            "roofline": {"bound": "int", "kernel": "k_bsgs", "achieved": bsgs_rate / 1e9, "peak": mmul_peak / 1e9,
+                         "unit": "G Montgomery-mul/s", "frac": bsgs_rate / mmul_peak if mmul_peak else None,
+                         "traffic": None, "imad_peak_gops": imad_peak / 1e9},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    siever.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,148 @@
+/*
+ * mps_gpu.h -- C-ABI of the B200 (sm_100a) Mass Prime Siever worker.
+ *
+ * Drop-in boundary for the GPU worker of Mass Prime Siever 14.0.  The
+ * reference binds its GPU through the C++ class GpuSiever
+ * ("Mass Prime Siever/Gpu.hpp":1040-1074) with two calls, sieve_filter and
+ * filter, made by process_chunk ("Mass Prime Siever/Worker.hpp":195-303).
+ * This header exposes the same two contracts as plain C functions, plus the
+ * exact relation path that moves run_bsgs ("Mass Prime Siever/Math.hpp":
+ * 377-486) onto the device, and a batched entry point for many items.
+ *
+ * Conventions: every function returns MPS_OK (0) or a negative MPS_E_* code;
+ * mps_last_error(ctx) gives the reason as text.  Buffers are caller-owned
+ * host memory; the library owns its device memory, allocated on demand and
+ * released by mps_close.  A context is used by one host thread at a time
+ * (the reference serialises its feeder threads with a mutex, Gpu.hpp:1059).
+ */
+#ifndef MPS_GPU_H
+#define MPS_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPS_ABI_VERSION 1
+
+enum {
+    MPS_OK = 0,
+    MPS_E_ARG = -1,       /* malformed arguments (NULL, P0 >= P1, res >= mod, ...)        */
+    MPS_E_RANGE = -2,     /* outside the GPU path: P1 > 2^62, lo <= 3 (compat), N1-N0 > 1e7 */
+    MPS_E_CAPACITY = -3,  /* the caller's output buffer is too small (*n_out = needed)     */
+    MPS_E_TIMEOUT = -4,   /* a bounded device wait expired                                */
+    MPS_E_CUDA = -5,      /* a CUDA call failed                                           */
+    MPS_E_NODEV = -6,     /* no usable CUDA device                                        */
+    MPS_E_STATE = -7      /* the context is closed or was poisoned by an earlier error    */
+};
+
+typedef struct mps_ctx mps_ctx;
+
+/* One Factor=b,c,P0,P1,N0,N1[,mod,res] line (Config.hpp:124-200, Types.hpp:14-26).
+ * b and c are signed 128-bit integers (two's complement, high word signed). */
+typedef struct mps_item {
+    int64_t  b_hi;
+    uint64_t b_lo;
+    int64_t  c_hi;
+    uint64_t c_lo;
+    uint64_t P0, P1;      /* primes P0 <= p < P1, P1 <= 2^62                 */
+    int64_t  N0, N1;      /* exponents N0 <= n < N1, N1 - N0 <= 10^7         */
+    uint64_t mod, res;    /* n == res (mod mod); mod 0 is taken as 1         */
+} mps_item;
+
+/* A relations.p line "p, M, q": p | b^n + c for n == M (mod q)
+ * (Math.hpp:360-364, Worker.hpp:294-297). */
+typedef struct mps_relation {
+    uint64_t p, M, q;
+} mps_relation;
+
+/* Tuning; zero fields take the defaults.  Every setting gives the same relations. */
+typedef struct mps_tuning {
+    uint32_t struct_size;       /* sizeof(mps_tuning)                                          */
+    uint32_t table_bits;        /* baby-step table of 2^bits slots per prime (0: per item)     */
+    uint64_t chunk_odds;        /* odd integers per device chunk (0: 2^26)                      */
+    uint32_t max_baby;          /* cap on the baby-step count (0: half the table)              */
+    uint32_t bsgs_warps;        /* warps per BSGS block (0: 4)                                 */
+    uint32_t class_modulus;     /* Q of the power-residue split g = gcd(Q, p-1) (0: lcm(mod,24)) */
+    uint32_t full_mr;           /* 1: 12-base Miller-Rabin on every filter survivor (eager)    */
+    uint32_t plain;             /* 1: plain per-chunk path (host sync between stages)          */
+    uint32_t reserved[7];
+} mps_tuning;
+
+/* Counters of the last call (all chunks of it). */
+typedef struct mps_stats {
+    uint64_t odds;              /* odd integers sieved                          */
+    uint64_t survivors;         /* survivors of the sieve by the primes <= 65521 */
+    uint64_t entries;           /* primes that reached the BSGS                 */
+    uint64_t relations;         /* relations returned                           */
+    uint64_t chunks;            /* device chunks run                            */
+    double   device_ms;         /* device time of the call (CUDA events)        */
+    double   bsgs_ms;           /* device time of the BSGS kernel               */
+    uint64_t bsgs_launches;
+    uint64_t kernel_launches;   /* kernels of this library launched             */
+    uint64_t bsgs_steps;        /* baby + giant steps (Montgomery multiplies) done by the BSGS */
+} mps_stats;
+
+/* ---- context (replaces CudaSiever::init, Cuda.hpp:198-257) ---- */
+int mps_tuning_default(mps_tuning* t);
+int mps_open(int device, const mps_tuning* tuning, mps_ctx** out);
+int mps_close(mps_ctx* ctx);
+const char* mps_last_error(const mps_ctx* ctx);
+int mps_get_stats(const mps_ctx* ctx, mps_stats* out);
+int mps_abi_version(void);
+
+/* ---- the exact path (new): run_bsgs on every prime of [lo, hi), on the device ----
+ * Relations of the primes lo <= p < hi, sorted by p.  0 <= lo < hi <= 2^62; the
+ * item's own P0/P1 are not consulted.  If cap is too small, returns
+ * MPS_E_CAPACITY with *n_out = the number needed.  Replaces the CPU loop of
+ * process_chunk (Worker.hpp:243-280) for one chunk. */
+int mps_chunk_relations(mps_ctx* ctx, uint64_t lo, uint64_t hi, const mps_item* item,
+                        mps_relation* out, size_t cap, size_t* n_out);
+
+/* All relations of one item, p over [P0, P1) (run_worker_pool, Worker.hpp:305-367). */
+int mps_item_relations(mps_ctx* ctx, const mps_item* item, mps_relation* out, size_t cap, size_t* n_out);
+
+/* ---- compat: GpuSiever::sieve_filter (Gpu.hpp:1064-1067, Cuda.hpp:329-415) ----
+ * Appends to out the numbers of [lo, hi) that may divide an in-class
+ * candidate: here exactly the primes with a relation, ascending.  Declines
+ * with MPS_E_RANGE unless hi < 2^62 and lo > 3 (Worker.hpp:209). */
+int mps_sieve_filter(mps_ctx* ctx, uint64_t lo, uint64_t hi, const mps_item* item,
+                     uint64_t* out, size_t cap, size_t* n_out);
+
+/* ---- compat: GpuSiever::filter (Gpu.hpp:1060-1063, Cuda.hpp:264-326) ----
+ * flags[i] = 1 when primes[i] may divide an in-class candidate (here: exactly
+ * when it has a relation), else 0.  primes[] are host-sieved primes. */
+int mps_filter(mps_ctx* ctx, const uint64_t* primes, size_t n, const mps_item* item, uint8_t* flags);
+
+/* ---- batched: many items through one persistent work-stealing launch per chunk ----
+ * Relations of every item over its [P0, P1); out_item[k] is the item index of
+ * out[k]; sorted by (item, p). */
+int mps_batch_relations(mps_ctx* ctx, const mps_item* items, size_t n_items, mps_relation* out,
+                        uint32_t* out_item, size_t cap, size_t* n_out);
+
+/* Number of primes in [lo, hi) counted on the device (the unit of the
+ * sieved-primes/s metric; not part of the relation path). */
+int mps_count_primes(mps_ctx* ctx, uint64_t lo, uint64_t hi, uint64_t* count);
+
+/* Arithmetic ceilings measured on this device: independent 64-bit Montgomery
+ * multiplies per second (the routine every BSGS step runs) and independent
+ * 32-bit integer multiply-adds per second (the integer pipe). */
+int mps_measure_peaks(mps_ctx* ctx, double* mmul_per_s, double* imad_per_s);
+
+/* ---- kernel-level hooks for parity tests ---- */
+/* Survivors of the odd sieve of [lo, hi) by the odd primes <= min(65521, sqrt(hi)), ascending. */
+int mps_test_survivors(mps_ctx* ctx, uint64_t lo, uint64_t hi, uint64_t* out, size_t cap, size_t* n_out);
+/* out[i] = is_prime64(n[i]) (Math.hpp:209-251), n[i] < 2^62. */
+int mps_test_is_prime(mps_ctx* ctx, const uint64_t* n, size_t count, uint8_t* out);
+/* cases[5k..5k+4] = p, B, G0, t, jcount: smallest j < jcount with G0*B^j == t (mod p),
+ * or UINT64_MAX; B, G0, t in [1, p). */
+int mps_test_bsgs(mps_ctx* ctx, const uint64_t* cases, size_t count, uint32_t table_bits, uint64_t* j_out);
+/* bp[2k], bp[2k+1] = b, p (p prime, p does not divide b): q_out[k] = ord_p(b) (Math.hpp:294-310). */
+int mps_test_order(mps_ctx* ctx, const uint64_t* bp, size_t count, uint64_t* q_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,177 @@
+// arith.cuh -- exact 64-bit modular arithmetic for the sm_100a kernels.
+//
+// Montgomery multiplication modulo an odd p < 2^62 with R = 2^64, written
+// for the integer multiply pipe: one 64x64->128 product, one 64-bit low
+// product and one high product per multiply.  Values are kept "lazy" in
+// [0, 2p): for a, b < 2p and p < 2^62, (a*b + m*p) / R < 2p, so no final
+// subtraction is needed between multiplies; norm() brings a value to [0, p)
+// where it is compared or hashed.  Same arithmetic as the reference's
+// Montgomery (Math.hpp:29-79) and mmul/mpow (Gpu.hpp:77-96), restated.
+#pragma once
+
+#include "mps_common.cuh"
+
+namespace mps {
+
+struct Mont {
+    u64 p;      // odd modulus, p < 2^62
+    u64 ninv;   // -p^-1 mod 2^64
+    u64 one;    // R mod p (the Montgomery form of 1)
+
+    // Newton iteration for p^-1 mod 2^64: 3p xor 2 is correct to 5 bits,
+    // each step doubles the correct bits (5 -> 10 -> 20 -> 40 -> 80).
+    __device__ __forceinline__ static u64 neg_inverse(u64 p) {
+        u64 inv = (3 * p) ^ 2;
+        inv *= 2 - p * inv;
+        inv *= 2 - p * inv;
+        inv *= 2 - p * inv;
+        inv *= 2 - p * inv;
+        return 0 - inv;
+    }
+
+    __device__ __forceinline__ void init(u64 modulus) {
+        p = modulus;
+        ninv = neg_inverse(modulus);
+        one = (0 - modulus) % modulus;
+    }
+
+    __device__ __forceinline__ u64 mul(u64 a, u64 b) const {
+        const u64 lo = a * b;
+        const u64 hi = __umul64hi(a, b);
+        const u64 m = lo * ninv;
+        const u64 mh = __umul64hi(m, p);
+        // lo + (m*p mod 2^64) is 0 (lo == 0) or exactly 2^64 (carry 1).
+        return hi + mh + (lo != 0 ? 1ull : 0ull);
+    }
+
+    __device__ __forceinline__ u64 norm(u64 a) const { return a >= p ? a - p : a; }
+
+    // 2a for a lazy value a < 2p, kept below 2p.
+    __device__ __forceinline__ u64 dbl(u64 a) const {
+        u64 x = a + a;
+        return x >= 2 * p ? x - 2 * p : x;
+    }
+
+    // R^2 mod p from R mod p: four doublings give 16R, four Montgomery
+    // squarings give 2^8 R, 2^16 R, 2^32 R, 2^64 R = R^2.
+    __device__ __forceinline__ u64 r2() const {
+        u64 a = one;
+        a = dbl(a); a = dbl(a); a = dbl(a); a = dbl(a);
+        a = mul(a, a); a = mul(a, a); a = mul(a, a); a = mul(a, a);
+        return norm(a);
+    }
+
+    __device__ __forceinline__ u64 to_mont(u64 a, u64 rr) const { return norm(mul(a, rr)); }
+    __device__ __forceinline__ u64 from_mont(u64 a) const { return norm(mul(a, 1)); }
+
+    // base^e (Montgomery form in and out, result normalised).
+    __device__ __forceinline__ u64 pow(u64 base, u64 e) const {
+        u64 r = one;
+        while (e) {
+            if (e & 1) r = mul(r, base);
+            base = mul(base, base);
+            e >>= 1;
+        }
+        return norm(r);
+    }
+};
+
+__device__ __forceinline__ u64 gcd64(u64 a, u64 b) {
+    while (b) {
+        const u64 t = a % b;
+        a = b;
+        b = t;
+    }
+    return a;
+}
+
+__device__ __forceinline__ u32 gcd32(u32 a, u32 b) {
+    while (b) {
+        const u32 t = a % b;
+        a = b;
+        b = t;
+    }
+    return a;
+}
+
+// Jacobi symbol (a/n) for odd n (binary algorithm, Gpu.hpp:213-226); strips
+// all factors of two of a at once.
+__device__ __forceinline__ int jacobi(u64 a, u64 n) {
+    u32 neg = 0;
+    while (a != 0) {
+        const int tz = __ffsll((long long)a) - 1;
+        a >>= tz;
+        const u32 n8 = (u32)n & 7u;
+        if ((tz & 1) && (n8 == 3u || n8 == 5u)) neg ^= 1u;
+        if (a < n) {
+            const u64 x = a;
+            a = n;
+            n = x;
+            if ((a & n & 3ull) == 3ull) neg ^= 1u;
+        }
+        a -= n;
+    }
+    return n == 1 ? (neg ? -1 : 1) : 0;
+}
+
+// Strong probable-prime test of p (odd, > 2) to base 2, in the Montgomery
+// form of `M`: 2^d by square-and-double.
+__device__ __forceinline__ bool sprp2(const Mont& M) {
+    const u64 p = M.p;
+    const u64 pm1 = p - 1;
+    const int s = __ffsll((long long)pm1) - 1;
+    const u64 d = pm1 >> s;
+    const u64 minus_one = p - M.one;
+    int k = 63 - __clzll((long long)d);
+    u64 x = M.dbl(M.one);          // 2^1 (top bit of d)
+    for (--k; k >= 0; --k) {
+        x = M.mul(x, x);
+        if ((d >> k) & 1) x = M.dbl(x);
+    }
+    x = M.norm(x);
+    if (x == M.one || x == minus_one) return true;
+    for (int r = 1; r < s; ++r) {
+        x = M.norm(M.mul(x, x));
+        if (x == minus_one) return true;
+        if (x == M.one) return false;
+    }
+    return false;
+}
+
+// Strong test to base a (a < p), Montgomery form.
+__device__ __forceinline__ bool sprp(const Mont& M, u64 a, u64 rr) {
+    const u64 pm1 = M.p - 1;
+    const int s = __ffsll((long long)pm1) - 1;
+    const u64 d = pm1 >> s;
+    const u64 minus_one = M.p - M.one;
+    u64 x = M.pow(M.to_mont(a, rr), d);
+    if (x == M.one || x == minus_one) return true;
+    for (int r = 1; r < s; ++r) {
+        x = M.norm(M.mul(x, x));
+        if (x == minus_one) return true;
+        if (x == M.one) return false;
+    }
+    return false;
+}
+
+// Exact deterministic primality for n < 2^62 (Math.hpp:209-251): trial
+// division by the 12 bases, then strong tests to the same 12 bases.
+__device__ __noinline__ bool is_prime64(u64 n) {
+    const u32 bases[12] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37};
+    if (n < 2) return false;
+    for (int i = 0; i < 12; ++i) {
+        if (n == bases[i]) return true;
+        if (n % bases[i] == 0) return false;
+    }
+    Mont M;
+    M.init(n);
+    const u64 rr = M.r2();
+    for (int i = 0; i < 12; ++i)
+        if (!sprp(M, bases[i], rr)) return false;
+    return true;
+}
+
+// Plain modular product for moduli below 2^32 (small-prime paths).
+__device__ __forceinline__ u64 mulmod_small(u64 a, u64 b, u64 p) { return (a * b) % p; }
+
+}  // namespace mps

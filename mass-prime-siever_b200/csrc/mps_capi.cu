@@ -1,0 +1,738 @@
+// mps_capi.cu -- the C-ABI of include/mps_gpu.h over the sm_100a kernels.
+//
+// A context owns one CUDA stream and its device buffers (allocated on
+// demand, grown when a chunk overflows them, freed by mps_close).  A chunk
+// of the prime range runs as sieve -> prep -> BSGS -> order on that stream;
+// in the default (persistent) mode the four kernels are queued back to back
+// and the host waits once per chunk, for the relation count.
+#include "../../include/mps_gpu.h"
+#include "mps_kernels.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace mps;
+
+namespace {
+
+constexpr u64 kTwo62 = 1ull << 62;
+constexpr u64 kMaxNSpan = 10000000ull;   // N1 - N0 <= 10^7 (Config.hpp:187-190)
+
+// Odd primes 3..65521 and their division constants.
+struct HostTables {
+    std::vector<u32> sp;
+    std::vector<u64> rcp, inv;
+    HostTables() {
+        std::vector<bool> comp(65536, false);
+        for (u32 i = 3; i < 65536; i += 2) {
+            if (comp[i]) continue;
+            sp.push_back(i);
+            for (u64 j = (u64)i * i; j < 65536; j += 2 * i) comp[j] = true;
+        }
+        for (u32 q : sp) {
+            rcp.push_back(~0ull / q);
+            u64 x = q;                       // q^-1 mod 2^64 by Newton
+            for (int k = 0; k < 6; ++k) x *= 2 - q * x;
+            inv.push_back(x);
+        }
+    }
+};
+
+const HostTables& host_tables() {
+    static const HostTables t;
+    return t;
+}
+
+u64 gcd_u64(u64 a, u64 b) {
+    while (b) {
+        const u64 t = a % b;
+        a = b;
+        b = t;
+    }
+    return a;
+}
+
+}  // namespace
+
+struct mps_ctx {
+    int device = 0;
+    int num_sms = 148;
+    size_t smem_optin = 227 * 1024;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evb0 = nullptr, evb1 = nullptr;
+    mps_tuning tun{};
+    std::string err;
+    bool poisoned = false;
+    mps_stats stats{};
+
+    u32* d_sp = nullptr;
+    u64* d_rcp = nullptr;
+    u64* d_inv = nullptr;
+    Counters* d_ctr = nullptr;
+    Counters* h_ctr = nullptr;      // pinned
+    u64* d_surv = nullptr;
+    u64 surv_cap = 0;
+    u32* d_surv_item = nullptr;
+    Entry* d_ent = nullptr;
+    u64 ent_cap = 0;
+    RawRelation* d_rel = nullptr;
+    RawRelation* h_rel = nullptr;   // pinned
+    u64 rel_cap = 0;
+    DevItem* d_items = nullptr;
+    u64 items_cap = 0;
+
+    SieveTables tables() const { return SieveTables{d_sp, d_rcp, d_inv}; }
+};
+
+namespace {
+
+int fail(mps_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_fail(mps_ctx* c, cudaError_t e, const char* what) {
+    c->poisoned = (e == cudaErrorIllegalAddress || e == cudaErrorLaunchFailure || e == cudaErrorIllegalInstruction ||
+                   e == cudaErrorMisalignedAddress || e == cudaErrorHardwareStackError);
+    return fail(c, MPS_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call, what)                                   \
+    do {                                                 \
+        cudaError_t e_ = (call);                         \
+        if (e_ != cudaSuccess) return cuda_fail(c, e_, what); \
+    } while (0)
+
+template <class T>
+int ensure(mps_ctx* c, T** ptr, u64* cap, u64 need, const char* what) {
+    if (*cap >= need && *ptr) return MPS_OK;
+    if (*ptr) CK(cudaFree(*ptr), "cudaFree");
+    *ptr = nullptr;
+    *cap = 0;
+    CK(cudaMalloc((void**)ptr, need * sizeof(T)), what);
+    *cap = need;
+    return MPS_OK;
+}
+
+int ensure_rel(mps_ctx* c, u64 need) {
+    if (c->rel_cap >= need && c->d_rel) return MPS_OK;
+    if (c->d_rel) CK(cudaFree(c->d_rel), "cudaFree");
+    if (c->h_rel) CK(cudaFreeHost(c->h_rel), "cudaFreeHost");
+    c->d_rel = nullptr;
+    c->h_rel = nullptr;
+    c->rel_cap = 0;
+    CK(cudaMalloc((void**)&c->d_rel, need * sizeof(RawRelation)), "relation buffer");
+    CK(cudaMallocHost((void**)&c->h_rel, need * sizeof(RawRelation)), "pinned relation buffer");
+    c->rel_cap = need;
+    return MPS_OK;
+}
+
+// Baby-step table size for the item: m <= ceil(sqrt(K)) (every prime's
+// j-range is at most K), load factor <= 1/2.
+void table_for(const mps_ctx* c, u64 K, u32* tbits, u32* max_baby) {
+    u32 tb = c->tun.table_bits;
+    if (tb == 0) {
+        u64 m = (u64)std::ceil(std::sqrt((double)std::max<u64>(K, 1)));
+        tb = 5;
+        while ((1ull << tb) < 2 * m && tb < 13) ++tb;
+    }
+    tb = std::min<u32>(std::max<u32>(tb, 5), 14);
+    u32 mb = c->tun.max_baby ? c->tun.max_baby : (1u << tb) / 2;
+    mb = std::min<u32>(std::min<u32>(mb, kMaxBaby), (1u << tb) - 1);
+    *tbits = tb;
+    *max_baby = std::max<u32>(mb, 1);
+}
+
+// Validates an item the way load_worktodo does (Config.hpp:156-190) plus the
+// GPU path's range (P1 <= 2^62); fills the device-side constants.
+int make_dev_item(mps_ctx* c, const mps_item* it, u32 index, DevItem* d) {
+    if (!it) return fail(c, MPS_E_ARG, "item is NULL");
+    if (it->P0 >= it->P1) return fail(c, MPS_E_ARG, "requires P0 < P1");
+    if (it->P1 > kTwo62) return fail(c, MPS_E_RANGE, "P1 must not exceed 2^62");
+    if (it->N0 >= it->N1) return fail(c, MPS_E_ARG, "requires N0 < N1");
+    if ((unsigned __int128)((__int128)it->N1 - it->N0) > kMaxNSpan) return fail(c, MPS_E_RANGE, "range N1-N0 exceeds 10 million");
+    const u64 cm = it->mod == 0 ? 1 : it->mod;
+    if (it->res >= cm) return fail(c, MPS_E_ARG, "class must satisfy 0 <= res < mod");
+    std::memset(d, 0, sizeof(*d));
+    const __int128 b = (__int128)(((unsigned __int128)(u64)it->b_hi << 64) | it->b_lo);
+    const __int128 cc = (__int128)(((unsigned __int128)(u64)it->c_hi << 64) | it->c_lo);
+    const unsigned __int128 babs = b < 0 ? (unsigned __int128)0 - (unsigned __int128)b : (unsigned __int128)b;
+    const unsigned __int128 cabs = cc < 0 ? (unsigned __int128)0 - (unsigned __int128)cc : (unsigned __int128)cc;
+    d->babs_hi = (u64)(babs >> 64);
+    d->babs_lo = (u64)babs;
+    d->cabs_hi = (u64)(cabs >> 64);
+    d->cabs_lo = (u64)cabs;
+    d->b_neg = b < 0;
+    d->c_neg = cc < 0;
+    d->N0_raw = it->N0;
+    d->N1_raw = it->N1;
+    d->N0 = it->N0 < 0 ? 0 : (u64)it->N0;
+    d->N1 = it->N1 < 0 ? 0 : (u64)it->N1;
+    d->cm = cm;
+    d->n_start = d->N0 + ((it->res % cm) + cm - (d->N0 % cm)) % cm;
+    d->has_work = (it->N1 > 0 && d->n_start < d->N1) ? 1 : 0;
+    d->K = d->has_work ? (d->N1 - d->n_start + cm - 1) / cm : 0;
+    u64 Q = c->tun.class_modulus;
+    if (Q == 0) {
+        const u64 l = cm / gcd_u64(cm, 24) * 24;
+        Q = l <= 1440 ? l : 24;
+    }
+    if (Q < 2 || Q > (1u << 20) || (Q & 1)) return fail(c, MPS_E_ARG, "class_modulus must be even and <= 2^20");
+    d->Q = (u32)Q;
+    d->Q_rcp = ~0ull / Q;
+    d->cmQ = (u32)(cm % Q);
+    d->nsQ = (u32)(d->n_start % Q);
+    d->item_index = index;
+    u32 tb = 0, mb = 0;
+    table_for(c, d->K, &tb, &mb);
+    d->max_baby = mb;
+    return MPS_OK;
+}
+
+u32 sieve_prime_count(u64 hi) {
+    const std::vector<u32>& sp = host_tables().sp;
+    u32 n = 0;
+    while (n < sp.size() && (u64)sp[n] * sp[n] < hi) ++n;
+    return n;
+}
+
+int upload_items(mps_ctx* c, const DevItem* items, size_t n) {
+    if (int r = ensure(c, &c->d_items, &c->items_cap, std::max<u64>(n, 1), "item buffer")) return r;
+    CK(cudaMemcpyAsync(c->d_items, items, n * sizeof(DevItem), cudaMemcpyHostToDevice, c->stream), "item upload");
+    return MPS_OK;
+}
+
+int grid_for(mps_ctx* c, int per_sm) { return c->num_sms * per_sm; }
+
+int bsgs_grid(mps_ctx* c, u32 tbits, u32 warps, int* grid) {
+    const size_t smem = bsgs_smem_bytes(tbits, warps);
+    if (smem > c->smem_optin) return fail(c, MPS_E_ARG, "baby-step tables exceed shared memory");
+    // blocks per SM limited by shared memory (1 KB reserved per block) and 64 warps per SM
+    int per_sm = (int)(228 * 1024 / (smem + 1024));
+    per_sm = std::min(per_sm, (int)(64 / warps));
+    per_sm = std::max(per_sm, 1);
+    *grid = c->num_sms * per_sm;
+    return MPS_OK;
+}
+
+// Relations of the primes of one device chunk [lo, hi) (at most chunk_odds
+// odd numbers) for item `item`, already on the device.  Appends RawRelations.
+int run_chunk(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, std::vector<RawRelation>& out) {
+    const u64 lo_odd = std::max<u64>(lo, 3) | 1ull;
+    const u64 n_odds = lo_odd < hi ? (hi - lo_odd + 1) / 2 : 0;
+    const u32 include_two = (lo <= 2 && hi > 2) ? 1 : 0;
+    if (n_odds == 0 && !include_two) return MPS_OK;
+    const u64 chunk = c->tun.chunk_odds;
+    const u64 need_surv = n_odds + 16;
+    if (int r = ensure(c, &c->d_surv, &c->surv_cap, std::max<u64>(need_surv, chunk + 16), "survivor buffer")) return r;
+    if (int r = ensure(c, &c->d_ent, &c->ent_cap, std::max<u64>(chunk / 4, 1 << 16), "entry buffer")) return r;
+    if (int r = ensure_rel(c, std::max<u64>(c->rel_cap, 1 << 18))) return r;
+
+    u32 tbits, max_baby;
+    table_for(c, K, &tbits, &max_baby);
+    (void)max_baby;
+    const u32 warps = c->tun.bsgs_warps ? c->tun.bsgs_warps : 4;
+
+    SieveArgs sa{};
+    sa.lo_odd = lo_odd;
+    sa.n_odds = n_odds;
+    sa.hi = hi;
+    sa.include_two = include_two;
+    sa.n_primes = sieve_prime_count(hi);
+    sa.item = item;
+
+    PrepArgs pa{};
+    pa.surv = c->d_surv;
+    pa.surv_cap = c->surv_cap;
+    pa.surv_item = nullptr;
+    pa.item0 = item;
+    pa.items = c->d_items;
+    pa.ent = c->d_ent;
+    pa.ent_cap = c->ent_cap;
+    pa.rel = c->d_rel;
+    pa.rel_cap = c->rel_cap;
+    pa.full_mr = c->tun.full_mr;
+
+    BsgsArgs ba{};
+    ba.ent = c->d_ent;
+    ba.ent_cap = c->ent_cap;
+    ba.rel = c->d_rel;
+    ba.rel_cap = c->rel_cap;
+    ba.tbits = tbits;
+    ba.warps_per_block = warps;
+
+    OrderArgs oa{};
+    oa.rel = c->d_rel;
+    oa.rel_cap = c->rel_cap;
+    oa.items = c->d_items;
+    oa.tables = c->tables();
+
+    cudaStream_t s = c->stream;
+    CK(cudaMemsetAsync(c->d_ctr, 0, sizeof(Counters), s), "counter reset");
+    CK(launch_sieve(sa, c->tables(), c->d_surv, nullptr, c->surv_cap, c->d_ctr, s), "sieve launch");
+    int bgrid = 0;
+    if (int r = bsgs_grid(c, tbits, warps, &bgrid)) return r;
+    if (c->tun.plain) {
+        // the plain path: a host read of each stage's count sizes the next launch
+        CK(cudaMemcpyAsync(c->h_ctr, c->d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, s), "count read");
+        CK(cudaStreamSynchronize(s), "sieve");
+        const u64 ns = std::min<u64>(c->h_ctr->survivors, c->surv_cap);
+        CK(launch_prep(pa, c->d_ctr, (int)std::max<u64>((ns + 255) / 256, 1), s), "prep launch");
+        CK(cudaMemcpyAsync(c->h_ctr, c->d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, s), "count read");
+        CK(cudaStreamSynchronize(s), "prep");
+        const u64 ne = std::min<u64>(c->h_ctr->entries, c->ent_cap);
+        ba.persistent = 0;
+        CK(cudaEventRecord(c->evb0, s), "event");
+        if (ne) CK(launch_bsgs(ba, c->d_ctr, (int)((ne + warps - 1) / warps), s), "bsgs launch");
+        CK(cudaEventRecord(c->evb1, s), "event");
+    } else {
+        CK(launch_prep(pa, c->d_ctr, grid_for(c, 16), s), "prep launch");
+        ba.persistent = 1;
+        CK(cudaEventRecord(c->evb0, s), "event");
+        CK(launch_bsgs(ba, c->d_ctr, bgrid, s), "bsgs launch");
+        CK(cudaEventRecord(c->evb1, s), "event");
+    }
+    CK(launch_order(oa, c->d_ctr, grid_for(c, 4), s), "order launch");
+    CK(cudaMemcpyAsync(c->h_ctr, c->d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, s), "count read");
+    CK(cudaStreamSynchronize(s), "chunk");
+    float bms = 0;
+    CK(cudaEventElapsedTime(&bms, c->evb0, c->evb1), "event time");
+    c->stats.bsgs_ms += bms;
+    c->stats.bsgs_launches += 1;
+    c->stats.kernel_launches += 4;
+    const Counters h = *c->h_ctr;
+    if (h.status & (kStatusSurvivorOverflow | kStatusEntryOverflow)) {
+        // a denser range than the buffers were sized for: halve the chunk
+        if (n_odds <= 1024) return fail(c, MPS_E_CUDA, "device buffers overflow on a tiny chunk");
+        const u64 mid = lo_odd + 2 * (n_odds / 2);
+        if (int r = run_chunk(c, lo, mid, item, K, out)) return r;
+        return run_chunk(c, mid, hi, item, K, out);
+    }
+    if (h.status & kStatusRelationOverflow) {
+        if (int r = ensure_rel(c, std::max<u64>(2 * c->rel_cap, h.relations + 1024))) return r;
+        return run_chunk(c, lo, hi, item, K, out);
+    }
+    if (h.status & kStatusOrderFailed) return fail(c, MPS_E_CUDA, "order computation did not factor p - 1");
+    const u64 nr = h.relations;
+    if (nr) {
+        CK(cudaMemcpyAsync(c->h_rel, c->d_rel, nr * sizeof(RawRelation), cudaMemcpyDeviceToHost, s), "relation read");
+        CK(cudaStreamSynchronize(s), "relation read");
+        for (u64 i = 0; i < nr; ++i)
+            if (c->h_rel[i].q != ~0ull) out.push_back(c->h_rel[i]);
+    }
+    c->stats.odds += n_odds;
+    c->stats.bsgs_steps += h.steps;
+    c->stats.survivors += h.survivors;
+    c->stats.entries += h.entries;
+    c->stats.chunks += 1;
+    return MPS_OK;
+}
+
+int check_ctx(mps_ctx* c) {
+    if (!c) return MPS_E_ARG;
+    if (c->poisoned) return fail(c, MPS_E_STATE, "context poisoned by an earlier device fault: " + c->err);
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaSetDevice");
+    return MPS_OK;
+}
+
+void begin_call(mps_ctx* c) {
+    std::memset(&c->stats, 0, sizeof(c->stats));
+    cudaEventRecord(c->ev0, c->stream);
+}
+
+int end_call(mps_ctx* c) {
+    CK(cudaEventRecord(c->ev1, c->stream), "event");
+    CK(cudaEventSynchronize(c->ev1), "event sync");
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1), "event time");
+    c->stats.device_ms = ms;
+    return MPS_OK;
+}
+
+// [lo, hi) in device chunks of at most chunk_odds odd numbers.
+int run_range(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, std::vector<RawRelation>& rel) {
+    const u64 chunk = c->tun.chunk_odds;
+    for (u64 a = lo; a < hi;) {
+        const u64 lo_odd = std::max<u64>(a, 3) | 1ull;
+        u64 b = hi;
+        if (lo_odd < hi && (hi - lo_odd + 1) / 2 > chunk) b = lo_odd + 2 * chunk;
+        if (int r = run_chunk(c, a, b, item, K, rel)) return r;
+        a = b;
+    }
+    return MPS_OK;
+}
+
+int relations_of(mps_ctx* c, const mps_item* item, u64 lo, u64 hi, std::vector<RawRelation>& rel) {
+    DevItem d;
+    if (int r = make_dev_item(c, item, 0, &d)) return r;
+    if (lo >= hi) return MPS_OK;
+    if (hi > kTwo62) return fail(c, MPS_E_RANGE, "hi must not exceed 2^62");
+    if (int r = upload_items(c, &d, 1)) return r;
+    return run_range(c, lo, hi, 0, d.K, rel);
+}
+
+void sort_by_p(std::vector<RawRelation>& rel) {
+    std::sort(rel.begin(), rel.end(), [](const RawRelation& a, const RawRelation& b) {
+        return a.item != b.item ? a.item < b.item : a.p < b.p;
+    });
+}
+
+int copy_out(mps_ctx* c, const std::vector<RawRelation>& rel, mps_relation* out, uint32_t* out_item, size_t cap,
+             size_t* n_out) {
+    if (n_out) *n_out = rel.size();
+    c->stats.relations = rel.size();
+    if (rel.size() > cap) return fail(c, MPS_E_CAPACITY, "output buffer too small");
+    for (size_t i = 0; i < rel.size(); ++i) {
+        out[i].p = rel[i].p;
+        out[i].M = rel[i].M;
+        out[i].q = rel[i].q;
+        if (out_item) out_item[i] = rel[i].item;
+    }
+    return MPS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mps_abi_version(void) { return MPS_ABI_VERSION; }
+
+int mps_tuning_default(mps_tuning* t) {
+    if (!t) return MPS_E_ARG;
+    std::memset(t, 0, sizeof(*t));
+    t->struct_size = sizeof(mps_tuning);
+    t->chunk_odds = 1ull << 26;
+    t->bsgs_warps = 4;
+    return MPS_OK;
+}
+
+int mps_open(int device, const mps_tuning* tuning, mps_ctx** out) {
+    if (!out) return MPS_E_ARG;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return MPS_E_NODEV;
+    if (device < 0 || device >= count) return MPS_E_NODEV;
+    mps_ctx* c = new mps_ctx();
+    c->device = device;
+    mps_tuning_default(&c->tun);
+    if (tuning) {
+        if (tuning->struct_size != sizeof(mps_tuning)) {
+            delete c;
+            return MPS_E_ARG;
+        }
+        const mps_tuning d = c->tun;
+        c->tun = *tuning;
+        if (!c->tun.chunk_odds) c->tun.chunk_odds = d.chunk_odds;
+        if (!c->tun.bsgs_warps) c->tun.bsgs_warps = d.bsgs_warps;
+    }
+    if (c->tun.chunk_odds < 4096) c->tun.chunk_odds = 4096;
+    auto bail = [&](cudaError_t e, const char* what) {
+        fprintf(stderr, "mps_open: %s: %s\n", what, cudaGetErrorString(e));
+        mps_close(c);
+        return MPS_E_CUDA;
+    };
+    cudaError_t e;
+    if ((e = cudaSetDevice(device)) != cudaSuccess) return bail(e, "cudaSetDevice");
+    cudaDeviceProp prop;
+    if ((e = cudaGetDeviceProperties(&prop, device)) != cudaSuccess) return bail(e, "properties");
+    c->num_sms = prop.multiProcessorCount;
+    c->smem_optin = prop.sharedMemPerBlockOptin;
+    if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "stream");
+    for (cudaEvent_t* ev : {&c->ev0, &c->ev1, &c->evb0, &c->evb1})
+        if ((e = cudaEventCreate(ev)) != cudaSuccess) return bail(e, "event");
+    const HostTables& t = host_tables();
+    const size_t n = t.sp.size();
+    if ((e = cudaMalloc((void**)&c->d_sp, n * sizeof(u32))) != cudaSuccess) return bail(e, "tables");
+    if ((e = cudaMalloc((void**)&c->d_rcp, n * sizeof(u64))) != cudaSuccess) return bail(e, "tables");
+    if ((e = cudaMalloc((void**)&c->d_inv, n * sizeof(u64))) != cudaSuccess) return bail(e, "tables");
+    if ((e = cudaMalloc((void**)&c->d_ctr, sizeof(Counters))) != cudaSuccess) return bail(e, "counters");
+    if ((e = cudaMallocHost((void**)&c->h_ctr, sizeof(Counters))) != cudaSuccess) return bail(e, "counters");
+    if ((e = cudaMemcpy(c->d_sp, t.sp.data(), n * sizeof(u32), cudaMemcpyHostToDevice)) != cudaSuccess) return bail(e, "upload");
+    if ((e = cudaMemcpy(c->d_rcp, t.rcp.data(), n * sizeof(u64), cudaMemcpyHostToDevice)) != cudaSuccess) return bail(e, "upload");
+    if ((e = cudaMemcpy(c->d_inv, t.inv.data(), n * sizeof(u64), cudaMemcpyHostToDevice)) != cudaSuccess) return bail(e, "upload");
+    *out = c;
+    return MPS_OK;
+}
+
+int mps_close(mps_ctx* c) {
+    if (!c) return MPS_E_ARG;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (void* p : {(void*)c->d_sp, (void*)c->d_rcp, (void*)c->d_inv, (void*)c->d_ctr, (void*)c->d_surv,
+                    (void*)c->d_surv_item, (void*)c->d_ent, (void*)c->d_rel, (void*)c->d_items})
+        if (p) cudaFree(p);
+    if (c->h_ctr) cudaFreeHost(c->h_ctr);
+    if (c->h_rel) cudaFreeHost(c->h_rel);
+    for (cudaEvent_t ev : {c->ev0, c->ev1, c->evb0, c->evb1})
+        if (ev) cudaEventDestroy(ev);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return MPS_OK;
+}
+
+const char* mps_last_error(const mps_ctx* c) { return c ? c->err.c_str() : "no context"; }
+
+int mps_get_stats(const mps_ctx* c, mps_stats* out) {
+    if (!c || !out) return MPS_E_ARG;
+    *out = c->stats;
+    return MPS_OK;
+}
+
+int mps_chunk_relations(mps_ctx* c, uint64_t lo, uint64_t hi, const mps_item* item, mps_relation* out, size_t cap,
+                        size_t* n_out) {
+    if (int r = check_ctx(c)) return r;
+    if (!out && cap) return fail(c, MPS_E_ARG, "out is NULL");
+    begin_call(c);
+    std::vector<RawRelation> rel;
+    if (int r = relations_of(c, item, lo, hi, rel)) return r;
+    if (int r = end_call(c)) return r;
+    sort_by_p(rel);
+    return copy_out(c, rel, out, nullptr, cap, n_out);
+}
+
+int mps_item_relations(mps_ctx* c, const mps_item* item, mps_relation* out, size_t cap, size_t* n_out) {
+    if (!item) return fail(c, MPS_E_ARG, "item is NULL");
+    return mps_chunk_relations(c, item->P0, item->P1, item, out, cap, n_out);
+}
+
+int mps_sieve_filter(mps_ctx* c, uint64_t lo, uint64_t hi, const mps_item* item, uint64_t* out, size_t cap,
+                     size_t* n_out) {
+    if (int r = check_ctx(c)) return r;
+    if (!(hi < kTwo62 && lo > 3)) return fail(c, MPS_E_RANGE, "the GPU sieve takes 3 < lo and hi < 2^62");
+    begin_call(c);
+    std::vector<RawRelation> rel;
+    if (int r = relations_of(c, item, lo, hi, rel)) return r;
+    if (int r = end_call(c)) return r;
+    sort_by_p(rel);
+    if (n_out) *n_out = rel.size();
+    c->stats.relations = rel.size();
+    if (rel.size() > cap) return fail(c, MPS_E_CAPACITY, "output buffer too small");
+    for (size_t i = 0; i < rel.size(); ++i) out[i] = rel[i].p;
+    return MPS_OK;
+}
+
+int mps_filter(mps_ctx* c, const uint64_t* primes, size_t n, const mps_item* item, uint8_t* flags) {
+    if (int r = check_ctx(c)) return r;
+    if (n == 0) return MPS_OK;
+    if (!primes || !flags) return fail(c, MPS_E_ARG, "NULL buffer");
+    DevItem d;
+    if (int r = make_dev_item(c, item, 0, &d)) return r;
+    for (size_t i = 0; i < n; ++i)
+        if (primes[i] >= kTwo62) return fail(c, MPS_E_RANGE, "primes must be below 2^62");
+    begin_call(c);
+    if (int r = upload_items(c, &d, 1)) return r;
+    const u64 chunk = c->tun.chunk_odds;
+    std::vector<RawRelation> rel;
+    for (size_t off = 0; off < n; off += chunk) {
+        const u64 cnt = std::min<u64>(chunk, n - off);
+        if (int r = ensure(c, &c->d_surv, &c->surv_cap, std::max<u64>(cnt + 16, chunk + 16), "survivor buffer")) return r;
+        if (int r = ensure(c, &c->d_ent, &c->ent_cap, std::max<u64>(cnt, 1 << 16), "entry buffer")) return r;
+        if (int r = ensure_rel(c, std::max<u64>(c->rel_cap, 1 << 18))) return r;
+        u32 tbits, mb;
+        table_for(c, d.K, &tbits, &mb);
+        const u32 warps = c->tun.bsgs_warps;
+        int bgrid = 0;
+        if (int r = bsgs_grid(c, tbits, warps, &bgrid)) return r;
+        cudaStream_t s = c->stream;
+        CK(cudaMemsetAsync(c->d_ctr, 0, sizeof(Counters), s), "counter reset");
+        CK(cudaMemcpyAsync(c->d_surv, primes + off, cnt * sizeof(u64), cudaMemcpyHostToDevice, s), "prime upload");
+        Counters h{};
+        h.survivors = cnt;
+        CK(cudaMemcpyAsync(&c->d_ctr->survivors, &h.survivors, sizeof(u64), cudaMemcpyHostToDevice, s), "count upload");
+        PrepArgs pa{};
+        pa.surv = c->d_surv; pa.surv_cap = c->surv_cap; pa.item0 = 0; pa.items = c->d_items;
+        pa.ent = c->d_ent; pa.ent_cap = c->ent_cap; pa.rel = c->d_rel; pa.rel_cap = c->rel_cap; pa.full_mr = c->tun.full_mr;
+        BsgsArgs ba{};
+        ba.ent = c->d_ent; ba.ent_cap = c->ent_cap; ba.rel = c->d_rel; ba.rel_cap = c->rel_cap;
+        ba.tbits = tbits; ba.warps_per_block = warps; ba.persistent = 1;
+        OrderArgs oa{};
+        oa.rel = c->d_rel; oa.rel_cap = c->rel_cap; oa.items = c->d_items; oa.tables = c->tables();
+        CK(launch_prep(pa, c->d_ctr, grid_for(c, 16), s), "prep launch");
+        CK(launch_bsgs(ba, c->d_ctr, bgrid, s), "bsgs launch");
+        CK(launch_order(oa, c->d_ctr, grid_for(c, 4), s), "order launch");
+        CK(cudaMemcpyAsync(c->h_ctr, c->d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, s), "count read");
+        CK(cudaStreamSynchronize(s), "filter");
+        if (c->h_ctr->status & (kStatusEntryOverflow | kStatusRelationOverflow | kStatusOrderFailed))
+            return fail(c, MPS_E_CUDA, "filter buffers overflowed");
+        const u64 nr = c->h_ctr->relations;
+        if (nr) {
+            CK(cudaMemcpy(c->h_rel, c->d_rel, nr * sizeof(RawRelation), cudaMemcpyDeviceToHost), "relation read");
+            for (u64 i = 0; i < nr; ++i)
+                if (c->h_rel[i].q != ~0ull) rel.push_back(c->h_rel[i]);
+        }
+        c->stats.kernel_launches += 3;
+    }
+    if (int r = end_call(c)) return r;
+    // flags by p (host-supplied primes may repeat or be unsorted)
+    std::vector<u64> ps;
+    ps.reserve(rel.size());
+    for (const RawRelation& r : rel) ps.push_back(r.p);
+    std::sort(ps.begin(), ps.end());
+    for (size_t i = 0; i < n; ++i) flags[i] = std::binary_search(ps.begin(), ps.end(), primes[i]) ? 1 : 0;
+    c->stats.relations = rel.size();
+    return MPS_OK;
+}
+
+int mps_batch_relations(mps_ctx* c, const mps_item* items, size_t n_items, mps_relation* out, uint32_t* out_item,
+                        size_t cap, size_t* n_out) {
+    if (int r = check_ctx(c)) return r;
+    if (!items && n_items) return fail(c, MPS_E_ARG, "items is NULL");
+    begin_call(c);
+    std::vector<RawRelation> rel;
+    std::vector<DevItem> d(n_items);
+    for (size_t i = 0; i < n_items; ++i)
+        if (int r = make_dev_item(c, &items[i], (u32)i, &d[i])) return r;
+    if (int r = upload_items(c, d.data(), n_items)) return r;
+    for (size_t i = 0; i < n_items; ++i)
+        if (int r = run_range(c, items[i].P0, items[i].P1, (u32)i, d[i].K, rel)) return r;
+    if (int r = end_call(c)) return r;
+    sort_by_p(rel);
+    return copy_out(c, rel, out, out_item, cap, n_out);
+}
+
+int mps_count_primes(mps_ctx* c, uint64_t lo, uint64_t hi, uint64_t* count) {
+    if (int r = check_ctx(c)) return r;
+    if (!count) return fail(c, MPS_E_ARG, "count is NULL");
+    if (hi > kTwo62) return fail(c, MPS_E_RANGE, "hi must not exceed 2^62");
+    *count = 0;
+    const u64 chunk = c->tun.chunk_odds;
+    for (u64 a = lo; a < hi;) {
+        const u64 lo_odd = std::max<u64>(a, 3) | 1ull;
+        u64 b = hi;
+        if (lo_odd < hi && (hi - lo_odd + 1) / 2 > chunk) b = lo_odd + 2 * chunk;
+        const u64 n_odds = lo_odd < b ? (b - lo_odd + 1) / 2 : 0;
+        if (int r = ensure(c, &c->d_surv, &c->surv_cap, chunk + 16, "survivor buffer")) return r;
+        SieveArgs sa{};
+        sa.lo_odd = lo_odd; sa.n_odds = n_odds; sa.hi = b; sa.include_two = (a <= 2 && b > 2);
+        sa.n_primes = sieve_prime_count(b);
+        CK(cudaMemsetAsync(c->d_ctr, 0, sizeof(Counters), c->stream), "counter reset");
+        CK(launch_sieve(sa, c->tables(), c->d_surv, nullptr, c->surv_cap, c->d_ctr, c->stream), "sieve launch");
+        CK(launch_count_primes(c->d_surv, c->surv_cap, c->d_ctr, grid_for(c, 8), c->stream), "count launch");
+        CK(cudaMemcpyAsync(c->h_ctr, c->d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, c->stream), "count read");
+        CK(cudaStreamSynchronize(c->stream), "count");
+        if (c->h_ctr->status) return fail(c, MPS_E_CUDA, "survivor buffer overflow while counting");
+        *count += c->h_ctr->primes;
+        a = b;
+    }
+    return MPS_OK;
+}
+
+int mps_measure_peaks(mps_ctx* c, double* mmul_per_s, double* imad_per_s) {
+    if (int r = check_ctx(c)) return r;
+    u64* sink = nullptr;
+    CK(cudaMalloc((void**)&sink, 64), "alloc");
+    const int grid = c->num_sms * 8;
+    const u32 iters = 4096;
+    float ms_m = 0, ms_i = 0;
+    cudaError_t e = cudaSuccess;
+    for (int rep = 0; rep < 3 && e == cudaSuccess; ++rep) {     // the last repetition is timed
+        e = cudaEventRecord(c->ev0, c->stream);
+        if (e == cudaSuccess) e = launch_mmul_peak(0x0000F00DF00D1ull, iters, grid, sink, c->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(c->ev1, c->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(c->ev1);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms_m, c->ev0, c->ev1);
+        if (e == cudaSuccess) e = cudaEventRecord(c->ev0, c->stream);
+        if (e == cudaSuccess) e = launch_imad_peak(iters * 8, grid, (u32*)sink, c->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(c->ev1, c->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(c->ev1);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms_i, c->ev0, c->ev1);
+    }
+    cudaFree(sink);
+    if (e != cudaSuccess) return cuda_fail(c, e, "peak probes");
+    const double threads = (double)grid * 256.0;
+    if (mmul_per_s) *mmul_per_s = threads * 8.0 * iters / (ms_m * 1e-3);
+    if (imad_per_s) *imad_per_s = threads * 8.0 * iters * 8.0 / (ms_i * 1e-3);
+    return MPS_OK;
+}
+
+int mps_test_survivors(mps_ctx* c, uint64_t lo, uint64_t hi, uint64_t* out, size_t cap, size_t* n_out) {
+    if (int r = check_ctx(c)) return r;
+    if (hi > kTwo62 || lo >= hi) return fail(c, MPS_E_RANGE, "need lo < hi <= 2^62");
+    const u64 lo_odd = std::max<u64>(lo, 3) | 1ull;
+    const u64 n_odds = lo_odd < hi ? (hi - lo_odd + 1) / 2 : 0;
+    if (n_odds > (1ull << 30)) return fail(c, MPS_E_RANGE, "range too wide for the test hook");
+    if (int r = ensure(c, &c->d_surv, &c->surv_cap, std::max<u64>(n_odds + 16, c->surv_cap), "survivor buffer")) return r;
+    SieveArgs sa{};
+    sa.lo_odd = lo_odd; sa.n_odds = n_odds; sa.hi = hi; sa.include_two = 0;
+    sa.n_primes = sieve_prime_count(hi);
+    CK(cudaMemsetAsync(c->d_ctr, 0, sizeof(Counters), c->stream), "counter reset");
+    CK(launch_sieve(sa, c->tables(), c->d_surv, nullptr, c->surv_cap, c->d_ctr, c->stream), "sieve launch");
+    CK(cudaMemcpyAsync(c->h_ctr, c->d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, c->stream), "count read");
+    CK(cudaStreamSynchronize(c->stream), "sieve");
+    const u64 ns = c->h_ctr->survivors;
+    if (n_out) *n_out = ns;
+    if (ns > cap) return fail(c, MPS_E_CAPACITY, "output buffer too small");
+    CK(cudaMemcpy(out, c->d_surv, ns * sizeof(u64), cudaMemcpyDeviceToHost), "survivor read");
+    std::sort(out, out + ns);
+    return MPS_OK;
+}
+
+int mps_test_is_prime(mps_ctx* c, const uint64_t* n, size_t count, uint8_t* out) {
+    if (int r = check_ctx(c)) return r;
+    for (size_t i = 0; i < count; ++i)
+        if (n[i] >= kTwo62) return fail(c, MPS_E_RANGE, "n must be below 2^62");
+    u64* dn = nullptr;
+    u32* dout = nullptr;
+    CK(cudaMalloc((void**)&dn, std::max<size_t>(count, 1) * sizeof(u64)), "alloc");
+    CK(cudaMalloc((void**)&dout, std::max<size_t>(count, 1) * sizeof(u32)), "alloc");
+    std::vector<u32> h(count);
+    cudaError_t e = cudaMemcpy(dn, n, count * sizeof(u64), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = launch_is_prime(dn, dout, count, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e == cudaSuccess) e = cudaMemcpy(h.data(), dout, count * sizeof(u32), cudaMemcpyDeviceToHost);
+    cudaFree(dn);
+    cudaFree(dout);
+    if (e != cudaSuccess) return cuda_fail(c, e, "is_prime test");
+    for (size_t i = 0; i < count; ++i) out[i] = (uint8_t)h[i];
+    return MPS_OK;
+}
+
+int mps_test_bsgs(mps_ctx* c, const uint64_t* cases, size_t count, uint32_t table_bits, uint64_t* j_out) {
+    if (int r = check_ctx(c)) return r;
+    if (table_bits < 5 || table_bits > 14) return fail(c, MPS_E_ARG, "table_bits must be in [5, 14]");
+    for (size_t i = 0; i < count; ++i) {
+        const uint64_t* k = cases + 5 * i;
+        if (k[0] < 3 || !(k[0] & 1) || k[0] >= kTwo62) return fail(c, MPS_E_RANGE, "p must be odd, 3 <= p < 2^62");
+        if (k[1] == 0 || k[1] >= k[0] || k[2] == 0 || k[2] >= k[0] || k[3] == 0 || k[3] >= k[0])
+            return fail(c, MPS_E_ARG, "B, G0, t must lie in [1, p)");
+    }
+    u64* dc = nullptr;
+    u64* dj = nullptr;
+    CK(cudaMalloc((void**)&dc, std::max<size_t>(count, 1) * 5 * sizeof(u64)), "alloc");
+    CK(cudaMalloc((void**)&dj, std::max<size_t>(count, 1) * sizeof(u64)), "alloc");
+    cudaError_t e = cudaMemcpy(dc, cases, count * 5 * sizeof(u64), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = launch_bsgs_direct(dc, dj, count, table_bits, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e == cudaSuccess) e = cudaMemcpy(j_out, dj, count * sizeof(u64), cudaMemcpyDeviceToHost);
+    cudaFree(dc);
+    cudaFree(dj);
+    if (e != cudaSuccess) return cuda_fail(c, e, "bsgs test");
+    return MPS_OK;
+}
+
+int mps_test_order(mps_ctx* c, const uint64_t* bp, size_t count, uint64_t* q_out) {
+    if (int r = check_ctx(c)) return r;
+    for (size_t i = 0; i < count; ++i) {
+        const u64 b = bp[2 * i], p = bp[2 * i + 1];
+        if (p < 3 || p >= kTwo62 || b % p == 0) return fail(c, MPS_E_ARG, "need 3 <= p < 2^62 and p not dividing b");
+    }
+    u64* db = nullptr;
+    u64* dq = nullptr;
+    CK(cudaMalloc((void**)&db, std::max<size_t>(count, 1) * 2 * sizeof(u64)), "alloc");
+    CK(cudaMalloc((void**)&dq, std::max<size_t>(count, 1) * sizeof(u64)), "alloc");
+    cudaError_t e = cudaMemcpy(db, bp, count * 2 * sizeof(u64), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = launch_order_direct(db, dq, count, c->tables(), c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e == cudaSuccess) e = cudaMemcpy(q_out, dq, count * sizeof(u64), cudaMemcpyDeviceToHost);
+    cudaFree(db);
+    cudaFree(dq);
+    if (e != cudaSuccess) return cuda_fail(c, e, "order test");
+    return MPS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,91 @@
+// mps_common.cuh -- shared types of the sm_100a siever kernels.
+//
+// Device-side layout of one Factor= work item, the BSGS entry handed from
+// the prep stage to the solve stage, and the relation record.  Everything is
+// plain 64-bit integer data; nothing here touches torch.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mps {
+
+typedef unsigned long long u64;
+typedef long long i64;
+typedef unsigned int u32;
+
+// Odd primes 3..65521 (6,541 of them): the sieving primes of the segment
+// sieve (same set as gpu_sieve_primes, Math.hpp:342-358).
+constexpr u32 kSievePrimes = 6541;
+constexpr u32 kSieveMaxPrime = 65521;
+
+// Largest baby-step count of one prime; the table entry keeps the baby index
+// in its low kIdxBits bits.
+constexpr u32 kIdxBits = 12;
+constexpr u32 kMaxBaby = (1u << kIdxBits) - 1;   // index 4095 is never used, so no entry equals kEmptySlot
+constexpr u32 kEmptySlot = 0xFFFFFFFFu;
+
+// Item constants, precomputed on the host once per item (all integer, exact).
+struct DevItem {
+    u64 babs_hi, babs_lo;  // |b| as 128-bit magnitude
+    u64 cabs_hi, cabs_lo;  // |c|
+    u32 b_neg, c_neg;      // signs
+    i64 N0_raw;            // N0 as given (the p | b relation reports it, Math.hpp:496-502)
+    i64 N1_raw;            // N1 as given (small-prime path, Math.hpp:506)
+    u64 N0;                // max(N0, 0)  (Math.hpp:390)
+    u64 N1;
+    u64 cm;                // class modulus (>= 1)
+    u64 n_start;           // smallest in-class n >= N0 (Math.hpp:393)
+    u64 K;                 // in-class n in [n_start, N1): n = n_start + cm*k, k < K
+    u32 has_work;          // K > 0
+    u32 Q;                 // power-residue split modulus: g = gcd(Q, p - 1)
+    u64 Q_rcp;             // floor((2^64 - 1) / Q)
+    u32 cmQ;               // cm mod Q
+    u32 nsQ;               // n_start mod Q
+    u32 max_baby;          // cap on the baby-step count m of this item (<= kMaxBaby)
+    u32 item_index;
+};
+
+// One prime that reached the discrete-log stage: solve G0 * B^j == t (mod p)
+// for the smallest j in [0, jcount).  Residues are in Montgomery form
+// (R = 2^64) and normalised to [0, p).
+struct Entry {
+    u64 p;
+    u64 ninv;             // -p^-1 mod 2^64
+    u64 one;              // R mod p
+    u64 t;                // -c
+    u64 G0;               // b^n_first
+    u64 B;                // b^L
+    u64 Bm;               // B^m
+    u64 n_first;          // smallest candidate n (n == R mod L, n >= N0)
+    u64 L;                // n = n_first + j*L
+    u64 jcount;
+    u32 m;                // baby steps (<= kMaxBaby)
+    u32 item;             // item index (batched runs)
+};
+
+// A relation before its order is known (q == 0 means "compute it").
+struct RawRelation {
+    u64 p, M, q;
+    u32 item;
+    u32 pad;
+};
+
+// Per-run device counters (one cache line each to keep atomics apart).
+struct Counters {
+    unsigned long long survivors;  u64 pad0[7];
+    unsigned long long entries;    u64 pad1[7];
+    unsigned long long relations;  u64 pad2[7];
+    unsigned long long work_next;  u64 pad3[7];
+    unsigned long long status;     u64 pad4[7];   // nonzero: an error bit set by a kernel
+    unsigned long long primes;     u64 pad5[7];   // prime count (counting kernel only)
+    unsigned long long steps;      u64 pad6[7];   // baby + giant steps executed by the BSGS
+};
+
+// Status bits a kernel may set (host turns them into error codes).
+constexpr u64 kStatusSurvivorOverflow = 1ull << 0;
+constexpr u64 kStatusEntryOverflow    = 1ull << 1;
+constexpr u64 kStatusRelationOverflow = 1ull << 2;
+constexpr u64 kStatusOrderFailed      = 1ull << 3;
+
+}  // namespace mps

@@ -1,0 +1,83 @@
+// mps_kernels.cuh -- launchers of the sm_100a siever kernels (mps_kernels.cu).
+#pragma once
+
+#include "mps_common.cuh"
+
+namespace mps {
+
+// Sieving-prime tables (device, built once per context).
+struct SieveTables {
+    const u32* sp;      // odd primes 3..65521
+    const u64* rcp;     // floor((2^64 - 1) / q)
+    const u64* inv;     // q^-1 mod 2^64
+};
+
+// Segment sieve of the odd numbers of [lo, hi) by the odd primes <= 65521:
+// every survivor (an odd v >= 3 with no odd prime factor q <= min(65521,
+// sqrt(hi)) other than itself) is appended to surv[].  include_two adds 2.
+struct SieveArgs {
+    u64 lo_odd;        // first odd >= max(lo, 3)
+    u64 n_odds;        // odd numbers to sieve
+    u64 hi;            // exclusive bound
+    u32 include_two;
+    u32 n_primes;      // sieving primes to use (those with q*q < hi, at most 6541)
+    u32 item;          // item index stored with the survivors
+};
+
+cudaError_t launch_sieve(const SieveArgs& a, const SieveTables& t, u64* surv, u32* surv_item, u64 surv_cap,
+                         Counters* ctr, cudaStream_t s);
+
+// Prep: filters, primality screen and BSGS set-up for every survivor.
+struct PrepArgs {
+    const u64* surv;
+    u64 surv_cap;
+    const u32* surv_item;      // nullptr: every survivor belongs to `item0`
+    u32 item0;
+    const DevItem* items;
+    Entry* ent;
+    u64 ent_cap;
+    RawRelation* rel;
+    u64 rel_cap;
+    u32 full_mr;               // 1: 12-base Miller-Rabin on every survivor that passes the filters
+};
+cudaError_t launch_prep(const PrepArgs& a, Counters* ctr, int grid, cudaStream_t s);
+
+// Exact BSGS, one warp per entry.
+struct BsgsArgs {
+    const Entry* ent;
+    u64 ent_cap;
+    RawRelation* rel;
+    u64 rel_cap;
+    u32 tbits;                 // baby-step table of 2^tbits slots per warp
+    u32 warps_per_block;
+    u32 persistent;            // 1: work-stealing warps; 0: one warp per entry
+    u64 max_entries;           // non-persistent grid size (entries launched)
+};
+cudaError_t launch_bsgs(const BsgsArgs& a, Counters* ctr, int grid, cudaStream_t s);
+
+// Order q = ord_p(b) and the exact 12-base primality check of every relation.
+struct OrderArgs {
+    RawRelation* rel;
+    u64 rel_cap;
+    const DevItem* items;
+    SieveTables tables;
+};
+cudaError_t launch_order(const OrderArgs& a, Counters* ctr, int grid, cudaStream_t s);
+
+// Counts the primes among the survivors (exact 12-base test) into ctr->primes.
+cudaError_t launch_count_primes(const u64* surv, u64 surv_cap, Counters* ctr, int grid, cudaStream_t s);
+
+// Roofline probes: 256 x grid threads x 8 independent chains x iters operations.
+cudaError_t launch_mmul_peak(u64 p, u32 iters, int grid, u64* sink, cudaStream_t s);
+cudaError_t launch_imad_peak(u32 iters, int grid, u32* sink, cudaStream_t s);
+
+// Test hooks: raw kernels on given inputs.
+cudaError_t launch_is_prime(const u64* n, u32* out, u64 count, cudaStream_t s);
+cudaError_t launch_bsgs_direct(const u64* cases /* p,B,G0,t,jcount */, u64* j_out, u64 count, u32 tbits,
+                               cudaStream_t s);
+cudaError_t launch_order_direct(const u64* bp /* b,p pairs */, u64* q_out, u64 count, SieveTables t,
+                                cudaStream_t s);
+
+size_t bsgs_smem_bytes(u32 tbits, u32 warps_per_block);
+
+}  // namespace mps

@@ -1,0 +1,259 @@
+"""ctypes binding of libmps_b200.so (the C-ABI of include/mps_gpu.h).
+
+Used by the tests, bench.py and __graft_entry__.py.  The product is the
+shared library and the C++ host (host/); this module only calls the C-ABI.
+It raises when the library is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmps_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "mps_gpu.h")
+U64_MAX = (1 << 64) - 1
+
+MPS_OK, MPS_E_ARG, MPS_E_RANGE, MPS_E_CAPACITY, MPS_E_TIMEOUT, MPS_E_CUDA, MPS_E_NODEV, MPS_E_STATE = \
+    0, -1, -2, -3, -4, -5, -6, -7
+ERROR_NAMES = {MPS_E_ARG: "MPS_E_ARG", MPS_E_RANGE: "MPS_E_RANGE", MPS_E_CAPACITY: "MPS_E_CAPACITY",
+               MPS_E_TIMEOUT: "MPS_E_TIMEOUT", MPS_E_CUDA: "MPS_E_CUDA", MPS_E_NODEV: "MPS_E_NODEV",
+               MPS_E_STATE: "MPS_E_STATE"}
+
+
+class MpsError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERROR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Item(ctypes.Structure):
+    _fields_ = [
+        ("b_hi", ctypes.c_int64), ("b_lo", ctypes.c_uint64),
+        ("c_hi", ctypes.c_int64), ("c_lo", ctypes.c_uint64),
+        ("P0", ctypes.c_uint64), ("P1", ctypes.c_uint64),
+        ("N0", ctypes.c_int64), ("N1", ctypes.c_int64),
+        ("mod", ctypes.c_uint64), ("res", ctypes.c_uint64),
+    ]
+
+
+class Relation(ctypes.Structure):
+    _fields_ = [("p", ctypes.c_uint64), ("M", ctypes.c_uint64), ("q", ctypes.c_uint64)]
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [
+        ("struct_size", ctypes.c_uint32), ("table_bits", ctypes.c_uint32),
+        ("chunk_odds", ctypes.c_uint64), ("max_baby", ctypes.c_uint32),
+        ("bsgs_warps", ctypes.c_uint32), ("class_modulus", ctypes.c_uint32),
+        ("full_mr", ctypes.c_uint32), ("plain", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 7),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("odds", ctypes.c_uint64), ("survivors", ctypes.c_uint64), ("entries", ctypes.c_uint64),
+        ("relations", ctypes.c_uint64), ("chunks", ctypes.c_uint64), ("device_ms", ctypes.c_double),
+        ("bsgs_ms", ctypes.c_double), ("bsgs_launches", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint64),
+        ("bsgs_steps", ctypes.c_uint64),
+    ]
+
+
+def split128(v: int) -> tuple[int, int]:
+    if not -(1 << 127) <= v < (1 << 127):
+        raise ValueError("value does not fit in a signed 128-bit integer")
+    u = v & ((1 << 128) - 1)
+    hi = u >> 64
+    if hi >= 1 << 63:
+        hi -= 1 << 64
+    return hi, u & U64_MAX
+
+
+def make_item(b: int, c: int, P0: int, P1: int, N0: int, N1: int, mod: int = 1, res: int = 0) -> Item:
+    bh, bl = split128(b)
+    ch, cl = split128(c)
+    return Item(bh, bl, ch, cl, P0, P1, N0, N1, mod, res)
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads the in-tree shared library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is not built: run `make -C mass-prime-siever_b200` (or build())")
+    L = ctypes.CDLL(path)
+    u64, u32, sz, P = ctypes.c_uint64, ctypes.c_uint32, ctypes.c_size_t, ctypes.POINTER
+    vp = ctypes.c_void_p
+    L.mps_tuning_default.argtypes = [P(Tuning)]
+    L.mps_open.argtypes = [ctypes.c_int, P(Tuning), P(vp)]
+    L.mps_close.argtypes = [vp]
+    L.mps_last_error.argtypes = [vp]
+    L.mps_last_error.restype = ctypes.c_char_p
+    L.mps_get_stats.argtypes = [vp, P(Stats)]
+    L.mps_chunk_relations.argtypes = [vp, u64, u64, P(Item), P(Relation), sz, P(sz)]
+    L.mps_item_relations.argtypes = [vp, P(Item), P(Relation), sz, P(sz)]
+    L.mps_sieve_filter.argtypes = [vp, u64, u64, P(Item), P(u64), sz, P(sz)]
+    L.mps_filter.argtypes = [vp, P(u64), sz, P(Item), P(ctypes.c_uint8)]
+    L.mps_batch_relations.argtypes = [vp, P(Item), sz, P(Relation), P(u32), sz, P(sz)]
+    L.mps_count_primes.argtypes = [vp, u64, u64, P(u64)]
+    L.mps_measure_peaks.argtypes = [vp, P(ctypes.c_double), P(ctypes.c_double)]
+    L.mps_test_survivors.argtypes = [vp, u64, u64, P(u64), sz, P(sz)]
+    L.mps_test_is_prime.argtypes = [vp, P(u64), sz, P(ctypes.c_uint8)]
+    L.mps_test_bsgs.argtypes = [vp, P(u64), sz, u32, P(u64)]
+    L.mps_test_order.argtypes = [vp, P(u64), sz, P(u64)]
+    _lib = L
+    return L
+
+
+def header_symbols(path: str = HEADER) -> list[str]:
+    """Function names declared in include/mps_gpu.h."""
+    text = open(path).read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*|void)\s+(mps_\w+)\s*\(", text, re.M)))
+
+
+def default_tuning(**kw) -> Tuning:
+    L = load_library()
+    t = Tuning()
+    L.mps_tuning_default(ctypes.byref(t))
+    for k, v in kw.items():
+        if not hasattr(t, k):
+            raise AttributeError(k)
+        setattr(t, k, v)
+    return t
+
+
+class Siever:
+    """One device context (mps_ctx).  Mirrors GpuSiever (Gpu.hpp:1040-1074):
+    sieve_filter / filter with the same contracts, plus the exact relation
+    calls.  Not thread-safe; serialise calls per instance."""
+
+    def __init__(self, device: int = 0, tuning: Tuning | None = None, **kw):
+        self.lib = load_library()
+        if tuning is None:
+            tuning = default_tuning(**kw)
+        self.ctx = ctypes.c_void_p()
+        rc = self.lib.mps_open(device, ctypes.byref(tuning), ctypes.byref(self.ctx))
+        if rc != MPS_OK:
+            raise MpsError(rc, "mps_open failed (no CUDA device?)")
+
+    def close(self):
+        if self.ctx:
+            self.lib.mps_close(self.ctx)
+            self.ctx = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int):
+        if rc != MPS_OK:
+            raise MpsError(rc, self.lib.mps_last_error(self.ctx).decode())
+
+    def stats(self) -> dict:
+        s = Stats()
+        self._check(self.lib.mps_get_stats(self.ctx, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+    def _relations(self, fn, *args, cap: int = 1 << 14):
+        while True:
+            buf = (Relation * max(cap, 1))()
+            n = ctypes.c_size_t()
+            rc = fn(self.ctx, *args, buf, cap, ctypes.byref(n))
+            if rc == MPS_E_CAPACITY:
+                cap = n.value
+                continue
+            self._check(rc)
+            return [(buf[i].p, buf[i].M, buf[i].q) for i in range(n.value)]
+
+    def chunk_relations(self, lo: int, hi: int, item: Item):
+        return self._relations(self.lib.mps_chunk_relations, lo, hi, ctypes.byref(item))
+
+    def item_relations(self, item: Item):
+        return self._relations(self.lib.mps_item_relations, ctypes.byref(item))
+
+    def sieve_filter(self, lo: int, hi: int, item: Item, cap: int = 1 << 14) -> list[int]:
+        while True:
+            buf = (ctypes.c_uint64 * max(cap, 1))()
+            n = ctypes.c_size_t()
+            rc = self.lib.mps_sieve_filter(self.ctx, lo, hi, ctypes.byref(item), buf, cap, ctypes.byref(n))
+            if rc == MPS_E_CAPACITY:
+                cap = n.value
+                continue
+            self._check(rc)
+            return list(buf[:n.value])
+
+    def filter(self, primes: list[int], item: Item) -> list[int]:
+        n = len(primes)
+        arr = (ctypes.c_uint64 * max(n, 1))(*primes)
+        flags = (ctypes.c_uint8 * max(n, 1))()
+        self._check(self.lib.mps_filter(self.ctx, arr, n, ctypes.byref(item), flags))
+        return list(flags[:n])
+
+    def batch_relations(self, items: list[Item], cap: int = 1 << 14):
+        arr = (Item * max(len(items), 1))(*items)
+        while True:
+            buf = (Relation * max(cap, 1))()
+            its = (ctypes.c_uint32 * max(cap, 1))()
+            n = ctypes.c_size_t()
+            rc = self.lib.mps_batch_relations(self.ctx, arr, len(items), buf, its, cap, ctypes.byref(n))
+            if rc == MPS_E_CAPACITY:
+                cap = n.value
+                continue
+            self._check(rc)
+            return [(its[i], buf[i].p, buf[i].M, buf[i].q) for i in range(n.value)]
+
+    def count_primes(self, lo: int, hi: int) -> int:
+        c = ctypes.c_uint64()
+        self._check(self.lib.mps_count_primes(self.ctx, lo, hi, ctypes.byref(c)))
+        return c.value
+
+    def measure_peaks(self) -> tuple[float, float]:
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.mps_measure_peaks(self.ctx, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def survivors(self, lo: int, hi: int, cap: int = 1 << 16) -> list[int]:
+        while True:
+            buf = (ctypes.c_uint64 * max(cap, 1))()
+            n = ctypes.c_size_t()
+            rc = self.lib.mps_test_survivors(self.ctx, lo, hi, buf, cap, ctypes.byref(n))
+            if rc == MPS_E_CAPACITY:
+                cap = n.value
+                continue
+            self._check(rc)
+            return list(buf[:n.value])
+
+    def is_prime(self, nums: list[int]) -> list[int]:
+        n = len(nums)
+        arr = (ctypes.c_uint64 * max(n, 1))(*nums)
+        out = (ctypes.c_uint8 * max(n, 1))()
+        self._check(self.lib.mps_test_is_prime(self.ctx, arr, n, out))
+        return list(out[:n])
+
+    def bsgs(self, cases: list[tuple[int, int, int, int, int]], table_bits: int = 12) -> list[int | None]:
+        flat = [x for c in cases for x in c]
+        arr = (ctypes.c_uint64 * max(len(flat), 1))(*flat)
+        out = (ctypes.c_uint64 * max(len(cases), 1))()
+        self._check(self.lib.mps_test_bsgs(self.ctx, arr, len(cases), table_bits, out))
+        return [None if out[i] == U64_MAX else out[i] for i in range(len(cases))]
+
+    def order(self, pairs: list[tuple[int, int]]) -> list[int]:
+        flat = [x for bp in pairs for x in bp]
+        arr = (ctypes.c_uint64 * max(len(flat), 1))(*flat)
+        out = (ctypes.c_uint64 * max(len(pairs), 1))()
+        self._check(self.lib.mps_test_order(self.ctx, arr, len(pairs), out))
+        return list(out[:len(pairs)])
