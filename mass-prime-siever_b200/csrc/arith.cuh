@@ -171,6 +171,65 @@ __device__ __noinline__ bool is_prime64(u64 n) {
     return true;
 }
 
+// Exact modular multiplication on the FP64 pipe for odd p < 2^49.
+//
+// Values are doubles holding integers; "lazy" values lie in (-2p, 2p) and a
+// product lands in (-p, p).  For |a|, |b| < 2p < 2^50:
+//   h = fl(a*b), l = fma(a, b, -h)          a*b = h + l exactly (|l| <= 2^46)
+//   q = nearest integer to h * fl(1/p)      via fma(h, pinv, 1.5*2^52) - 1.5*2^52
+//   r = fma(-q, p, h)                       exact: h - q*p is an integer, |.| <= 0.75p
+//   r + l                                   exact, == a*b (mod p), |.| <= p
+// (|h*pinv| < 2^51 keeps the rounding trick exact.)  Every operation uses an
+// explicit round-to-nearest intrinsic so that nothing is contracted or
+// reassociated.  A zero product never occurs in the solve (all values are
+// units), so |r + l| < p there and one conditional +p gives [0, p).
+struct Fp64 {
+    double p, pinv;
+    u64 pi;
+
+    __device__ __forceinline__ void init(u64 modulus) {
+        pi = modulus;
+        p = (double)modulus;
+        pinv = __ddiv_rn(1.0, p);
+    }
+    __device__ __forceinline__ double mul(double a, double b) const {
+        const double C = 6755399441055744.0;   // 1.5 * 2^52
+        const double h = __dmul_rn(a, b);
+        const double l = __fma_rn(a, b, -h);
+        const double q = __dsub_rn(__fma_rn(h, pinv, C), C);
+        const double r = __fma_rn(-q, p, h);
+        return __dadd_rn(r, l);
+    }
+    // [0, p) representative of a value in (-p, p).
+    __device__ __forceinline__ double canon(double a) const {
+        if (a < 0.0) a = __dadd_rn(a, p);
+        return a;
+    }
+    // The integer of a canonical value (exact: a + 2^52 < 2^53).
+    __device__ __forceinline__ u64 bits(double a) const {
+        return (u64)__double_as_longlong(__dadd_rn(a, 4503599627370496.0)) & ((1ull << 52) - 1);
+    }
+    __device__ __forceinline__ double from_u64(u64 x) const { return (double)x; }   // x < p < 2^49: exact
+    __device__ __forceinline__ double one() const { return 1.0; }
+    // Exact [0, p) residue of any lazy value in (-2p, 2p) (prep paths, zero allowed).
+    __device__ __forceinline__ u64 residue(double a) const {
+        double x = a;
+        if (x < 0.0) x = __dadd_rn(x, p);
+        if (x < 0.0) x = __dadd_rn(x, p);
+        if (x >= p) x = __dsub_rn(x, p);
+        return (u64)x;
+    }
+    __device__ __forceinline__ double pow(double base, u64 e) const {
+        double r = 1.0;
+        while (e) {
+            if (e & 1) r = mul(r, base);
+            base = mul(base, base);
+            e >>= 1;
+        }
+        return r;
+    }
+};
+
 // Plain modular product for moduli below 2^32 (small-prime paths).
 __device__ __forceinline__ u64 mulmod_small(u64 a, u64 b, u64 p) { return (a * b) % p; }
 

@@ -131,17 +131,19 @@ int ensure_rel(mps_ctx* c, u64 need) {
     return MPS_OK;
 }
 
-// Baby-step table size for the item: m <= ceil(sqrt(K)) (every prime's
-// j-range is at most K), load factor <= 1/2.
+// Baby-step table size for the item.  Every prime's j-range is at most K;
+// the table load is kept near 1/5 (a probe then reads one slot) and at most
+// 2^12 slots (8-16 KB per warp keeps ~24 warps resident per SM), so wide N
+// ranges trade baby steps for giant steps.
 void table_for(const mps_ctx* c, u64 K, u32* tbits, u32* max_baby) {
+    const u64 m_opt = (u64)std::ceil(std::sqrt((double)std::max<u64>(K, 1)));
     u32 tb = c->tun.table_bits;
     if (tb == 0) {
-        u64 m = (u64)std::ceil(std::sqrt((double)std::max<u64>(K, 1)));
-        tb = 5;
-        while ((1ull << tb) < 2 * m && tb < 13) ++tb;
+        tb = 6;
+        while ((1ull << tb) < 5 * m_opt && tb < 11) ++tb;
     }
     tb = std::min<u32>(std::max<u32>(tb, 5), 14);
-    u32 mb = c->tun.max_baby ? c->tun.max_baby : (1u << tb) / 2;
+    u32 mb = c->tun.max_baby ? c->tun.max_baby : std::max<u32>((1u << tb) / 5, 1);
     mb = std::min<u32>(std::min<u32>(mb, kMaxBaby), (1u << tb) - 1);
     *tbits = tb;
     *max_baby = std::max<u32>(mb, 1);
@@ -178,12 +180,24 @@ int make_dev_item(mps_ctx* c, const mps_item* it, u32 index, DevItem* d) {
     d->K = d->has_work ? (d->N1 - d->n_start + cm - 1) / cm : 0;
     u64 Q = c->tun.class_modulus;
     if (Q == 0) {
-        const u64 l = cm / gcd_u64(cm, 24) * 24;
-        Q = l <= 1440 ? l : 24;
+        // the split modulus: 5040 = 2^4 3^2 5 7 (and the class modulus, when small)
+        const u64 l = cm / gcd_u64(cm, 5040) * 5040;
+        Q = l <= 100800 ? l : 5040;
     }
     if (Q < 2 || Q > (1u << 20) || (Q & 1)) return fail(c, MPS_E_ARG, "class_modulus must be even and <= 2^20");
+    // (at most 7 distinct prime factors below 2^20: 2*3*5*7*11*13*17 = 510510)
     d->Q = (u32)Q;
     d->Q_rcp = ~0ull / Q;
+    {
+        u64 x = Q;
+        d->qf_n = 0;
+        for (u64 l = 2; l * l <= x; ++l) {
+            if (x % l) continue;
+            d->qf_l[d->qf_n++] = (u32)l;
+            while (x % l == 0) x /= l;
+        }
+        if (x > 1) d->qf_l[d->qf_n++] = (u32)x;
+    }
     d->cmQ = (u32)(cm % Q);
     d->nsQ = (u32)(d->n_start % Q);
     d->item_index = index;
@@ -264,6 +278,8 @@ int run_chunk(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, std::vector<RawRelati
     ba.rel_cap = c->rel_cap;
     ba.tbits = tbits;
     ba.warps_per_block = warps;
+    ba.chains = c->tun.reserved[0] ? c->tun.reserved[0] : 2;
+    ba.max_p = hi;
 
     OrderArgs oa{};
     oa.rel = c->d_rel;
@@ -431,6 +447,7 @@ int mps_open(int device, const mps_tuning* tuning, mps_ctx** out) {
         if (!c->tun.bsgs_warps) c->tun.bsgs_warps = d.bsgs_warps;
     }
     if (c->tun.chunk_odds < 4096) c->tun.chunk_odds = 4096;
+    if (c->tun.bsgs_warps > 8) c->tun.bsgs_warps = 8;       // the BSGS kernel is built for <= 256 threads per block
     auto bail = [&](cudaError_t e, const char* what) {
         fprintf(stderr, "mps_open: %s: %s\n", what, cudaGetErrorString(e));
         mps_close(c);
@@ -549,7 +566,8 @@ int mps_filter(mps_ctx* c, const uint64_t* primes, size_t n, const mps_item* ite
         pa.ent = c->d_ent; pa.ent_cap = c->ent_cap; pa.rel = c->d_rel; pa.rel_cap = c->rel_cap; pa.full_mr = c->tun.full_mr;
         BsgsArgs ba{};
         ba.ent = c->d_ent; ba.ent_cap = c->ent_cap; ba.rel = c->d_rel; ba.rel_cap = c->rel_cap;
-        ba.tbits = tbits; ba.warps_per_block = warps; ba.persistent = 1;
+        ba.tbits = tbits; ba.warps_per_block = warps; ba.persistent = 1; ba.chains = 2;
+        ba.max_p = *std::max_element(primes + off, primes + off + cnt);
         OrderArgs oa{};
         oa.rel = c->d_rel; oa.rel_cap = c->rel_cap; oa.items = c->d_items; oa.tables = c->tables();
         CK(launch_prep(pa, c->d_ctr, grid_for(c, 16), s), "prep launch");

@@ -19,11 +19,8 @@ typedef unsigned int u32;
 constexpr u32 kSievePrimes = 6541;
 constexpr u32 kSieveMaxPrime = 65521;
 
-// Largest baby-step count of one prime; the table entry keeps the baby index
-// in its low kIdxBits bits.
-constexpr u32 kIdxBits = 12;
-constexpr u32 kMaxBaby = (1u << kIdxBits) - 1;   // index 4095 is never used, so no entry equals kEmptySlot
-constexpr u32 kEmptySlot = 0xFFFFFFFFu;
+// Largest baby-step count of one prime (a table of 2^13 slots at load 1/2).
+constexpr u32 kMaxBaby = 4096;
 
 // Item constants, precomputed on the host once per item (all integer, exact).
 struct DevItem {
@@ -44,20 +41,19 @@ struct DevItem {
     u32 nsQ;               // n_start mod Q
     u32 max_baby;          // cap on the baby-step count m of this item (<= kMaxBaby)
     u32 item_index;
+    u32 qf_n;              // prime factors of Q: qf_l[0..qf_n)
+    u32 qf_l[7];
 };
 
 // One prime that reached the discrete-log stage: solve G0 * B^j == t (mod p)
-// for the smallest j in [0, jcount).  Residues are in Montgomery form
-// (R = 2^64) and normalised to [0, p).
+// for the smallest j in [0, jcount).  Plain residues in [0, p).
 struct Entry {
     u64 p;
-    u64 ninv;             // -p^-1 mod 2^64
-    u64 one;              // R mod p
     u64 t;                // -c
     u64 G0;               // b^n_first
     u64 B;                // b^L
     u64 Bm;               // B^m
-    u64 n_first;          // smallest candidate n (n == R mod L, n >= N0)
+    u64 n_first;          // smallest candidate n (n == r mod L, n >= N0)
     u64 L;                // n = n_first + j*L
     u64 jcount;
     u32 m;                // baby steps (<= kMaxBaby)

@@ -3,9 +3,10 @@
 //   k_sieve  segment sieve of the odd numbers by the odd primes <= 65521,
 //            bitmap in shared memory, survivors compacted to global memory
 //            (what psieve does, Gpu.hpp:385-455, sized for 148 SMs)
-//   k_prep   per survivor: residues of b and -c, quadratic-character filter
-//            (Jacobi), base-2 strong test, power-residue split over
-//            g = gcd(Q, p - 1) (Gpu.hpp:465-589, Math.hpp:410-433), BSGS set-up
+//   k_prep   per survivor: residues of b and -c, base-2 strong test,
+//            power-residue split over g = gcd(Q, p - 1) (Gpu.hpp:465-589,
+//            Math.hpp:410-433), BSGS set-up; staged through shared-memory
+//            queues so that every stage runs with full warps
 //   k_bsgs   exact baby-step giant-step, one warp per prime: baby-step table
 //            of fingerprints + indices in shared memory, giant steps probed by
 //            every lane, the smallest j found with a warp min-reduction
@@ -22,6 +23,10 @@
 namespace mps {
 
 constexpr u32 FULL = 0xFFFFFFFFu;
+
+#ifndef MPS_BSGS_MINB
+#define MPS_BSGS_MINB 3      // resident 256-thread BSGS blocks per SM the register budget is cut for
+#endif
 
 // ---------------------------------------------------------------- helpers --
 
@@ -218,6 +223,45 @@ __global__ void __launch_bounds__(kSieveThreads) k_sieve(SieveArgs a, SieveTable
     }
 }
 
+// ------------------------------------------------------------ the fields --
+
+// Two exact arithmetics behind one interface: FP64 (p < 2^49, the FP64 pipe)
+// and 64-bit Montgomery (p < 2^62, the integer pipe).  V is the value type;
+// key() gives the canonical integer (the table key) of a canonical value.
+constexpr u64 kFp64Limit = 1ull << 49;
+
+struct FieldF {
+    typedef double V;
+    Fp64 f;
+    __device__ __forceinline__ void init(u64 p) { f.init(p); }
+    __device__ __forceinline__ V mul(V a, V b) const { return f.mul(a, b); }
+    __device__ __forceinline__ V canon(V a) const { return f.canon(a); }          // units: (-p, p) -> [0, p)
+    __device__ __forceinline__ u64 key(V c) const { return f.bits(c); }
+    __device__ __forceinline__ u64 residue(V a) const { return f.residue(a); }   // any lazy value
+    __device__ __forceinline__ V from_u64(u64 x) const { return (double)x; }
+    __device__ __forceinline__ V one() const { return 1.0; }
+    __device__ __forceinline__ V dbl(V a) const { return __dadd_rn(a, a); }      // (-p, p) -> (-2p, 2p)
+    __device__ __forceinline__ V pow(V b, u64 e) const { return f.pow(b, e); }
+};
+
+struct FieldM {
+    typedef u64 V;
+    Mont M;
+    u64 rr;
+    __device__ __forceinline__ void init(u64 p) {
+        M.init(p);
+        rr = M.r2();
+    }
+    __device__ __forceinline__ V mul(V a, V b) const { return M.mul(a, b); }
+    __device__ __forceinline__ V canon(V a) const { return M.norm(a); }
+    __device__ __forceinline__ u64 key(V c) const { return c; }
+    __device__ __forceinline__ u64 residue(V a) const { return M.from_mont(a); }
+    __device__ __forceinline__ V from_u64(u64 x) const { return M.to_mont(x, rr); }
+    __device__ __forceinline__ V one() const { return M.one; }
+    __device__ __forceinline__ V dbl(V a) const { return M.dbl(a); }
+    __device__ __forceinline__ V pow(V b, u64 e) const { return M.pow(b, e); }
+};
+
 // --------------------------------------------------------------- the prep --
 
 // p < 1000: the reference's direct BSGS over n in [0, m*m), m = ceil(sqrt(min(p, N1)))
@@ -237,74 +281,151 @@ __device__ void small_prime(u64 p, u64 b_mod, u64 t, const DevItem& it, const Pr
     }
 }
 
-__device__ void prep_one(u64 p, const DevItem& it, const PrepArgs& a, Counters* ctr) {
-    const u64 b_mod = residue128(it.babs_hi, it.babs_lo, it.b_neg, p);
+// Strong probable-prime test to base 2 in field F (square-and-double).
+template <class F>
+__device__ __forceinline__ bool sprp2_f(const F& f, u64 p) {
+    const u64 pm1 = p - 1;
+    const int s = __ffsll((long long)pm1) - 1;
+    const u64 d = pm1 >> s;
+    int k = 63 - __clzll((long long)d);
+    typename F::V x = f.dbl(f.one());               // 2 (top bit of d)
+    for (--k; k >= 0; --k) {
+        x = f.mul(x, x);
+        if ((d >> k) & 1) x = f.dbl(x);
+    }
+    u64 y = f.residue(x);
+    if (y == 1 || y == pm1) return true;
+    for (int r = 1; r < s; ++r) {
+        x = f.mul(x, x);
+        y = f.residue(x);
+        if (y == pm1) return true;
+        if (y == 1) return false;
+    }
+    return false;
+}
+
+// Residues of b and -c for the survivor p, and the cases that never reach
+// the field arithmetic: p | b (Math.hpp:383-385, 496-503), p < 1000
+// (Math.hpp:488-542), p | c or no candidate n (Math.hpp:386-396).
+// Returns true when p continues to the main path.
+__device__ __forceinline__ bool prep_special(u64 p, const DevItem& it, const PrepArgs& a, Counters* ctr, u64& b_mod,
+                                             u64& t) {
+    b_mod = residue128(it.babs_hi, it.babs_lo, it.b_neg, p);
     const u64 c_mod = residue128(it.cabs_hi, it.cabs_lo, it.c_neg, p);
-    const u64 t = c_mod == 0 ? 0 : p - c_mod;           // -c mod p
-    if (b_mod == 0) {                                   // p | b (Math.hpp:383-385, 496-503)
+    t = c_mod == 0 ? 0 : p - c_mod;                     // -c mod p
+    if (b_mod == 0) {
         if (t == 0) emit_relation(p, (u64)it.N0_raw, 1, it.item_index, a.rel, a.rel_cap, ctr);
-        return;
+        return false;
     }
     if (p < 1000) {
         small_prime(p, b_mod, t, it, a, ctr);
-        return;
+        return false;
     }
-    if (t == 0 || !it.has_work) return;                 // Math.hpp:386-396
+    return t != 0 && it.has_work;
+}
 
-    // Quadratic character: b^n == t needs (b/p)^n == (t/p).
-    const int jb = jacobi(b_mod, p), jt = jacobi(t, p);
-    if (jb == 0 || jt == 0) return;                     // a common factor: p is composite
-    int par = -1;                                       // forced parity of n, -1: none
-    if (jb == 1) {
-        if (jt != 1) return;
-    } else {
-        par = jt == 1 ? 0 : 1;
-        if (!(it.cm & 1) && (int)(it.n_start & 1) != par) return;
-    }
+// e = (p - 1) / g exactly, g | p - 1.
+__device__ __forceinline__ u64 exact_quotient(u64 pm1, u32 g) {
+    const int tz = __ffs(g) - 1;
+    return (pm1 >> tz) * (0 - Mont::neg_inverse((u64)(g >> tz)));
+}
 
-    Mont M;
-    M.init(p);
-    if (!sprp2(M)) return;                              // composite survivor
-    if (a.full_mr && !is_prime64(p)) return;
-    const u64 rr = M.r2();
-    const u64 bm = M.to_mont(b_mod, rr), tm = M.to_mont(t, rr);
-
-    // Power-residue split: with g = gcd(Q, p - 1), e = (p - 1) / g,
-    // w = b^e and u = t^e are g-th roots of unity and b^n == t forces
-    // w^n == u, i.e. n == r (mod d) with d = ord(w), or no solution.
-    u32 d = 1, r = 0;
-    const u64 pm1 = p - 1;
+__device__ __forceinline__ u32 gcd_Q(const DevItem& it, u64 pm1) {
     const u64 qh = __umul64hi(pm1, it.Q_rcp);
     u32 rem = (u32)(pm1 - qh * it.Q);
     if (rem >= it.Q) rem -= it.Q;
-    const u32 g = gcd32(it.Q, rem);
-    if (g > 2) {
-        const int tz = __ffs(g) - 1;
-        const u64 go = g >> tz;
-        const u64 e = (pm1 >> tz) * (0 - Mont::neg_inverse(go));   // exact (p - 1) / g
-        const u64 u = M.pow(tm, e), w = M.pow(bm, e);
-        u64 x = M.one;
+    return gcd32(it.Q, rem);
+}
+
+// Stage 2: with g = gcd(Q, p - 1) and e = (p - 1) / g, w = b^e and u = t^e
+// are g-th roots of unity and b^n == t forces w^n == u, i.e. n == r (mod d),
+// d = ord(w) -- or there is no solution.  Returns 0 (no solution), 1 (d, r
+// found by a walk of at most `walk` steps) or 2 (longer: deferred).
+template <class F>
+__device__ __forceinline__ int power_split(const F& f, u64 p, u64 b_mod, u64 t, const DevItem& it, u32 walk, u32& d,
+                                           u32& r) {
+    typedef typename F::V V;
+    const u64 pm1 = p - 1;
+    const u32 g = gcd_Q(it, pm1);
+    const u64 e = exact_quotient(pm1, g);
+    V u = f.one(), w = f.one(), bu = f.from_u64(t), bw = f.from_u64(b_mod);
+    for (u64 x = e; x; x >>= 1) {                      // two exponentiations, interleaved
+        if (x & 1) {
+            u = f.mul(u, bu);
+            w = f.mul(w, bw);
+        }
+        bu = f.mul(bu, bu);
+        bw = f.mul(bw, bw);
+    }
+    const u64 uk = f.residue(u);
+    V x = f.one();
+    bool found = false;
+    const u32 lim = min(g, walk);
+    for (u32 k = 0; k < lim; ++k) {                    // discrete log in <w>
+        if (!found && f.residue(x) == uk) {
+            r = k;
+            found = true;
+        }
+        x = f.mul(x, w);
+        if (f.residue(x) == 1) {
+            d = k + 1;
+            return found ? 1 : 0;
+        }
+    }
+    return lim == g ? 0 : 2;
+}
+
+// Stage 2b (rare): the same split for long orders, one prime power of g at a
+// time: w_l = w^(g/l^c), u_l = u^(g/l^c) in the l^c-th roots of unity, a walk
+// of at most l^c steps each, combined by the Chinese remainder theorem.
+template <class F>
+__device__ bool power_split_pp(const F& f, u64 p, u64 b_mod, u64 t, const DevItem& it, u32& d, u32& r) {
+    typedef typename F::V V;
+    const u64 pm1 = p - 1;
+    const u32 g = gcd_Q(it, pm1);
+    const u64 e = exact_quotient(pm1, g);
+    const V w = f.pow(f.from_u64(b_mod), e), u = f.pow(f.from_u64(t), e);
+    d = 1;
+    r = 0;
+    for (u32 i = 0; i < it.qf_n; ++i) {
+        const u32 l = it.qf_l[i];
+        if (g % l) continue;
+        u32 lc = l;
+        while (g % (lc * l) == 0) lc *= l;
+        const u32 k = g / lc;
+        const V wl = f.pow(w, k), ul = f.pow(u, k);
+        const u64 uk = f.residue(ul);
+        V x = f.one();
         bool found = false;
-        d = g;
-        for (u32 k = 0; k < g; ++k) {
-            if (!found && x == u) {
-                r = k;
+        u32 xr = 0, dl = lc;
+        for (u32 y = 0; y < lc; ++y) {
+            if (!found && f.residue(x) == uk) {
+                xr = y;
                 found = true;
             }
-            x = M.norm(M.mul(x, w));
-            if (x == M.one) {
-                d = k + 1;
+            x = f.mul(x, wl);
+            if (f.residue(x) == 1) {
+                dl = y + 1;
                 break;
             }
         }
-        if (!found) return;
-    } else if (par >= 0) {
-        d = 2;
-        r = (u32)par;
+        if (!found) return false;
+        // r' == r (mod d), r' == xr (mod dl); d, dl coprime
+        u32 step = 0;                                      // d * dl <= g <= Q < 2^21
+        while ((r + d * step) % dl != xr) ++step;
+        r += d * step;
+        d *= dl;
     }
+    return true;
+}
 
-    // n = n_start + cm*k (in class) with cm*k == r - n_start (mod d).
-    const u32 cmd = it.cmQ % d;
+// Stage 3: n = n_start + cm*k (in class) with n == r (mod d); the BSGS set-up
+// for G0 * B^j == t, G0 = b^n_first, B = b^L, j < jcount.
+template <class F>
+__device__ void bsgs_setup(const F& f, u64 p, u64 b_mod, u64 t, const DevItem& it, u32 d, u32 r, const PrepArgs& a,
+                           Counters* ctr) {
+    typedef typename F::V V;
+    const u32 cmd = it.cmQ % d;                        // d | Q
     const u32 want = (r + d - it.nsQ % d) % d;
     u32 k0 = 0, acc = 0;
     bool ok = false;
@@ -317,115 +438,269 @@ __device__ void prep_one(u64 p, const DevItem& it, const PrepArgs& a, Counters* 
         if (acc >= d) acc -= d;
     }
     if (!ok || k0 >= it.K) return;
-    const u32 per = d / gcd32(d, cmd);                  // period of k
+    const u32 per = d / gcd32(d, cmd);                 // period of k
     u64 jcount = ((u32)it.K - k0 + per - 1) / per;     // K < 2^32 (N1 - N0 <= 10^7)
-    if (jcount > p) jcount = p;                         // ord(B) < p (Math.hpp:398-400)
+    if (jcount > p) jcount = p;                        // ord(B) < p (Math.hpp:398-400)
     const u64 L = it.cm * per;
     const u64 n_first = it.n_start + it.cm * k0;
-
-    const u64 G0 = M.pow(bm, n_first);
-    if (G0 == tm) {                                     // j = 0
+    const V bv = f.from_u64(b_mod);
+    const u64 G0 = f.residue(f.pow(bv, n_first));
+    if (G0 == t) {                                     // j = 0
         emit_relation(p, n_first, 0, it.item_index, a.rel, a.rel_cap, ctr);
         return;
     }
     if (jcount <= 1) return;
-    const u64 B = M.pow(bm, L);
+    const V Bv = f.pow(bv, L);
     u32 m = (u32)isqrt_ceil_dev(jcount);
     if (m > it.max_baby) m = it.max_baby;
-    const u64 Bm = M.pow(B, m);
-
+    const u64 Bm = f.residue(f.pow(Bv, m));
     const u64 slot = atomicAdd(&ctr->entries, 1ull);
     if (slot >= a.ent_cap) {
         atomicOr(&ctr->status, kStatusEntryOverflow);
         return;
     }
     Entry e;
-    e.p = p; e.ninv = M.ninv; e.one = M.one; e.t = tm; e.G0 = G0; e.B = B; e.Bm = Bm;
+    e.p = p; e.t = t; e.G0 = G0; e.B = f.residue(Bv); e.Bm = Bm;
     e.n_first = n_first; e.L = L; e.jcount = jcount; e.m = m; e.item = it.item_index;
     a.ent[slot] = e;
 }
 
-__global__ void __launch_bounds__(256) k_prep(PrepArgs a, Counters* ctr) {
+template <class F>
+__device__ __forceinline__ bool stage1(u64 p, const PrepArgs& a) {
+    F f;
+    f.init(p);
+    if (!sprp2_f(f, p)) return false;
+    return !a.full_mr || is_prime64(p);
+}
+
+constexpr u32 kPrepThreads = 256;
+constexpr u32 kPrepBatch = 1024;
+constexpr u32 kWalk = 48;                              // stage-2 walk before deferring
+
+// Warp-aggregated push onto a shared-memory queue.
+__device__ __forceinline__ u32 queue_slot(u32* count, bool want) {
+    const u32 bal = __ballot_sync(FULL, want);
+    if (!bal) return 0;
+    const u32 lane = threadIdx.x & 31;
+    const int leader = __ffs(bal) - 1;
+    u32 base = 0;
+    if ((int)lane == leader) base = atomicAdd(count, __popc(bal));
+    base = __shfl_sync(FULL, base, leader);
+    return base + __popc(bal & ((1u << lane) - 1));
+}
+
+// The prep: one persistent kernel; each block takes batches of kPrepBatch
+// survivors through four stages separated by shared-memory queues, so that
+// every stage runs with full warps.
+__global__ void __launch_bounds__(kPrepThreads) k_prep(PrepArgs a, Counters* ctr) {
+    __shared__ u64 q_p[kPrepBatch];
+    __shared__ u32 q_item[kPrepBatch];
+    __shared__ u32 q_d[kPrepBatch];                    // d, r after stage 2
+    __shared__ u32 q_r[kPrepBatch];
+    __shared__ u64 d_p[kPrepBatch];                    // deferred to stage 2b
+    __shared__ u32 d_item[kPrepBatch];
+    __shared__ u32 n_q, n_q2, n_d;
+    __shared__ u64 q2_p[kPrepBatch];
+    __shared__ u32 q2_item[kPrepBatch];
     const u64 n = min((u64)*(volatile unsigned long long*)&ctr->survivors, a.surv_cap);
-    for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
-        const u32 item = a.surv_item ? a.surv_item[i] : a.item0;
-        prep_one(a.surv[i], a.items[item], a, ctr);
+    const u32 tid = threadIdx.x;
+    for (u64 b0 = (u64)blockIdx.x * kPrepBatch; b0 < n; b0 += (u64)gridDim.x * kPrepBatch) {
+        const u32 nb = (u32)min((u64)kPrepBatch, n - b0);
+        if (tid == 0) n_q = n_q2 = n_d = 0;
+        __syncthreads();
+        // stage 1: special cases, then the base-2 strong test
+        for (u32 k = tid; k < kPrepBatch; k += kPrepThreads) {
+            bool keep = false;
+            u64 p = 0;
+            u32 item = a.item0;
+            if (k < nb) {
+                p = a.surv[b0 + k];
+                if (a.surv_item) item = a.surv_item[b0 + k];
+                u64 bm, t;
+                if (prep_special(p, a.items[item], a, ctr, bm, t))
+                    keep = p < kFp64Limit ? stage1<FieldF>(p, a) : stage1<FieldM>(p, a);
+            }
+            const u32 s = queue_slot(&n_q, keep);
+            if (keep) {
+                q_p[s] = p;
+                q_item[s] = item;
+            }
+        }
+        __syncthreads();
+        // stage 2: power-residue split with a short walk
+        const u32 nq = n_q;
+        for (u32 k = tid; k < ((nq + 31) & ~31u); k += kPrepThreads) {
+            int res = 0;
+            u32 d = 1, r = 0;
+            u64 p = 0;
+            u32 item = 0;
+            if (k < nq) {
+                p = q_p[k];
+                item = q_item[k];
+                const DevItem& it = a.items[item];
+                const u64 bm = residue128(it.babs_hi, it.babs_lo, it.b_neg, p);
+                const u64 cm_ = residue128(it.cabs_hi, it.cabs_lo, it.c_neg, p);
+                const u64 t = p - cm_;
+                if (p < kFp64Limit) {
+                    FieldF f;
+                    f.init(p);
+                    res = power_split(f, p, bm, t, it, kWalk, d, r);
+                } else {
+                    FieldM f;
+                    f.init(p);
+                    res = power_split(f, p, bm, t, it, kWalk, d, r);
+                }
+            }
+            const u32 s2 = queue_slot(&n_q2, res == 1);
+            if (res == 1) {
+                q2_p[s2] = p;
+                q2_item[s2] = item;
+                q_d[s2] = d;
+                q_r[s2] = r;
+            }
+            const u32 sd = queue_slot(&n_d, res == 2);
+            if (res == 2) {
+                d_p[sd] = p;
+                d_item[sd] = item;
+            }
+        }
+        __syncthreads();
+        // stage 2b: long orders, one prime power at a time
+        const u32 nd = n_d;
+        for (u32 k = tid; k < ((nd + 31) & ~31u); k += kPrepThreads) {
+            bool ok = false;
+            u32 d = 1, r = 0;
+            u64 p = 0;
+            u32 item = 0;
+            if (k < nd) {
+                p = d_p[k];
+                item = d_item[k];
+                const DevItem& it = a.items[item];
+                const u64 bm = residue128(it.babs_hi, it.babs_lo, it.b_neg, p);
+                const u64 t = p - residue128(it.cabs_hi, it.cabs_lo, it.c_neg, p);
+                if (p < kFp64Limit) {
+                    FieldF f;
+                    f.init(p);
+                    ok = power_split_pp(f, p, bm, t, it, d, r);
+                } else {
+                    FieldM f;
+                    f.init(p);
+                    ok = power_split_pp(f, p, bm, t, it, d, r);
+                }
+            }
+            const u32 s2 = queue_slot(&n_q2, ok);
+            if (ok) {
+                q2_p[s2] = p;
+                q2_item[s2] = item;
+                q_d[s2] = d;
+                q_r[s2] = r;
+            }
+        }
+        __syncthreads();
+        // stage 3: class combination and the BSGS set-up
+        const u32 nq2 = n_q2;
+        for (u32 k = tid; k < nq2; k += kPrepThreads) {
+            const u64 p = q2_p[k];
+            const DevItem& it = a.items[q2_item[k]];
+            const u64 bm = residue128(it.babs_hi, it.babs_lo, it.b_neg, p);
+            const u64 t = p - residue128(it.cabs_hi, it.cabs_lo, it.c_neg, p);
+            const u32 d = q_d[k], r = q_r[k];
+            if (p < kFp64Limit) {
+                FieldF f;
+                f.init(p);
+                bsgs_setup(f, p, bm, t, it, d, r, a, ctr);
+            } else {
+                FieldM f;
+                f.init(p);
+                bsgs_setup(f, p, bm, t, it, d, r, a, ctr);
+            }
+        }
+        __syncthreads();
     }
 }
 
 // --------------------------------------------------------------- the BSGS --
+//
+// One warp per prime.  The baby-step table holds a 16-bit fingerprint per
+// slot (0 = empty; linear probing); a giant value whose fingerprint matches
+// is resolved exactly by recomputing the baby steps, which is rare (true
+// solutions, and fingerprint collisions at ~2^-15 per compare).
 
-__device__ __forceinline__ u32 table_slot(u64 v, u32 tbits, u32& fp) {
-    const u32 lo = (u32)v, hi = (u32)(v >> 32);
-    const u32 x = lo ^ (hi * 0x9E3779B1u);
-    fp = x & 0xFFFFFu;
-    return (x * 0x85EBCA6Bu) >> (32 - tbits);
+__device__ __forceinline__ void table_hash(u64 key, u32 tbits, u32& slot, u32& fp) {
+    const u32 lo = (u32)key, hi = (u32)(key >> 32);
+    const u32 x = (lo ^ (hi * 0x9E3779B1u)) * 0x85EBCA6Bu;
+    slot = x >> (32 - tbits);
+    fp = (x & 0xFFFFu) | 1u;
 }
 
-__device__ __forceinline__ void table_insert(u32* tab, u32 mask, u32 tbits, u64 v, u32 i) {
-    u32 fp;
-    u32 s = table_slot(v, tbits, fp);
-    const u32 entry = (fp << kIdxBits) | i;
-    while (atomicCAS(&tab[s], kEmptySlot, entry) != kEmptySlot) s = (s + 1) & mask;
+__device__ __forceinline__ void table_insert(unsigned short* tab, u32 mask, u32 tbits, u64 key) {
+    u32 s, fp;
+    table_hash(key, tbits, s, fp);
+    while (atomicCAS(&tab[s], (unsigned short)0, (unsigned short)fp) != 0) s = (s + 1) & mask;
 }
 
-// t * B^i == v ?  (exact check of a fingerprint match)
-__device__ __noinline__ bool verify_baby(const Mont& M, u64 t, u64 B, u32 i, u64 v) {
-    return M.norm(M.mul(t, M.pow(B, i))) == v;
-}
-
-// Smallest j = g*m - i over the table entries matching v (a giant value of
-// step g); ~0u when none matches exactly.
-__device__ __forceinline__ u32 table_probe(const u32* tab, u32 mask, u32 tbits, u64 v, u64 g, u32 m,
-                                           const Mont& M, u64 t, u64 B) {
-    u32 fp;
-    u32 s = table_slot(v, tbits, fp);
-    u32 best = ~0u;
+__device__ __forceinline__ bool table_maybe(const unsigned short* tab, u32 mask, u32 tbits, u64 key) {
+    u32 s, fp;
+    table_hash(key, tbits, s, fp);
     for (;;) {
         const u32 e = tab[s];
-        if (e == kEmptySlot) break;
-        if ((e >> kIdxBits) == fp) {
-            const u32 i = e & ((1u << kIdxBits) - 1);
-            if (verify_baby(M, t, B, i, v)) {
-                const u32 j = (u32)(g * m - i);
-                best = min(best, j);
-            }
-        }
+        if (e == fp) return true;
+        if (e == 0) return false;
         s = (s + 1) & mask;
     }
-    return best;
+}
+
+// Smallest i in [lo, limit) with key(t * B^i) == key, or -1 (warp-cooperative;
+// tbl = t * B^lane, B32 = B^32).
+template <class F>
+__device__ __noinline__ int find_baby_index(const F& f, typename F::V tbl, typename F::V B32, u32 lo, u32 limit, u64 key) {
+    const u32 lane = threadIdx.x & 31;
+    typename F::V v = tbl;
+    for (u32 base = 0; base < limit; base += 32) {
+        const u32 i = base + lane;
+        const bool hit = i >= lo && i < limit && f.key(f.canon(v)) == key;
+        const u32 bal = __ballot_sync(FULL, hit);
+        if (bal) return (int)(base + __ffs(bal) - 1);
+        v = f.mul(v, B32);
+    }
+    return -1;
 }
 
 // Solves one entry with the 32 lanes of the calling warp; returns the
 // smallest j (< jcount) or ~0ull.  Two interleaved chains per lane: baby
 // indices i = l + 64k and l + 32 + 64k, giant steps g = 1 + l + 64k and
 // 33 + l + 64k.
-__device__ u64 solve_entry(const Entry& e, u32* tab, u32 tbits, u64* steps_out = nullptr) {
+template <class F>
+__device__ u64 solve_entry(const Entry& e, unsigned short* tab, u32 tbits, u64* steps_out) {
+    typedef typename F::V V;
     const u32 lane = threadIdx.x & 31;
-    Mont M;
-    M.p = e.p; M.ninv = e.ninv; M.one = e.one;
+    F f;
+    f.init(e.p);
     const u32 m = e.m;
     const u32 T = 1u << tbits, mask = T - 1;
+    const V B = f.from_u64(e.B), Bm = f.from_u64(e.Bm), tv = f.from_u64(e.t), G0 = f.from_u64(e.G0);
+    const u64 tkey = f.key(f.canon(tv));
 
     // lane powers by an inclusive scan: xb = B^(l+1), xg = Bm^(l+1)
-    u64 xb = e.B, xg = e.Bm;
+    V xb = B, xg = Bm;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
-        const u64 yb = __shfl_up_sync(FULL, xb, off), yg = __shfl_up_sync(FULL, xg, off);
+        const V yb = __shfl_up_sync(FULL, xb, off), yg = __shfl_up_sync(FULL, xg, off);
         if (lane >= (u32)off) {
-            xb = M.mul(xb, yb);
-            xg = M.mul(xg, yg);
+            xb = f.mul(xb, yb);
+            xg = f.mul(xg, yg);
         }
     }
-    const u64 B32 = __shfl_sync(FULL, xb, 31), Bm32 = __shfl_sync(FULL, xg, 31);
-    u64 bl = __shfl_up_sync(FULL, xb, 1);
-    if (lane == 0) bl = M.one;                          // B^l
-    const u64 B64 = M.mul(B32, B32), Bm64 = M.mul(Bm32, Bm32);
-    u64 baby0 = M.mul(e.t, bl), baby1 = M.mul(baby0, B32);
-    u64 gi0 = M.mul(e.G0, xg), gi1 = M.mul(gi0, Bm32);
+    const V B32 = __shfl_sync(FULL, xb, 31), Bm32 = __shfl_sync(FULL, xg, 31);
+    V bl = __shfl_up_sync(FULL, xb, 1);
+    if (lane == 0) bl = f.one();                       // B^l
+    const V B64 = f.mul(B32, B32), Bm64 = f.mul(Bm32, Bm32);
+    const V tbl = f.mul(tv, bl);                       // t B^l
+    V baby0 = tbl, baby1 = f.mul(tbl, B32);
+    V gi0 = f.mul(G0, xg), gi1 = f.mul(gi0, Bm32);
 
     uint4* t4 = reinterpret_cast<uint4*>(tab);
-    for (u32 k = lane; k < T / 4; k += 32) t4[k] = make_uint4(kEmptySlot, kEmptySlot, kEmptySlot, kEmptySlot);
+    for (u32 k = lane; k < T / 8; k += 32) t4[k] = make_uint4(0, 0, 0, 0);
     __syncwarp();
 
     // baby steps t*B^i, stopping at a cycle B^d == 1 (d < m)
@@ -433,20 +708,20 @@ __device__ u64 solve_entry(const Entry& e, u32* tab, u32 tbits, u64* steps_out =
     u64 steps = 0;
     for (u32 base = 0; base < m; base += 64) {
         const u32 i0 = base + lane, i1 = base + 32 + lane;
-        const u64 v0 = M.norm(baby0), v1 = M.norm(baby1);
-        const u32 b0 = __ballot_sync(FULL, i0 > 0 && i0 < m && v0 == e.t);
-        const u32 b1 = __ballot_sync(FULL, i1 < m && v1 == e.t);
+        const u64 k0 = f.key(f.canon(baby0)), k1 = f.key(f.canon(baby1));
+        const u32 b0 = __ballot_sync(FULL, i0 > 0 && i0 < m && k0 == tkey);
+        const u32 b1 = __ballot_sync(FULL, i1 < m && k1 == tkey);
         u32 lim = m;
         if (b0 | b1) {
             cyc = b0 ? base + __ffs(b0) - 1 : base + 32 + __ffs(b1) - 1;
             lim = cyc;
         }
-        if (i0 < lim) table_insert(tab, mask, tbits, v0, i0);
-        if (i1 < lim) table_insert(tab, mask, tbits, v1, i1);
+        if (i0 < lim) table_insert(tab, mask, tbits, k0);
+        if (i1 < lim) table_insert(tab, mask, tbits, k1);
         steps += min(64u, lim - base);
         if (cyc) break;
-        baby0 = M.mul(baby0, B64);
-        baby1 = M.mul(baby1, B64);
+        baby0 = f.mul(baby0, B64);
+        baby1 = f.mul(baby1, B64);
     }
     __syncwarp();
 
@@ -454,36 +729,38 @@ __device__ u64 solve_entry(const Entry& e, u32* tab, u32 tbits, u64* steps_out =
     if (cyc) {
         // ord(B) = cyc < m: the answer is the j in [1, cyc) with G0 == t*B^(cyc-j)
         // (j = 0 was ruled out by the prep); t*B^i, i < cyc, are distinct.
-        u32 jl = ~0u;
-        if (lane == 0) {
-            u32 fp;
-            u32 s = table_slot(e.G0, tbits, fp);
-            for (;;) {
-                const u32 en = tab[s];
-                if (en == kEmptySlot) break;
-                const u32 i = en & ((1u << kIdxBits) - 1);
-                if ((en >> kIdxBits) == fp && i >= 1 && i < cyc && verify_baby(M, e.t, e.B, i, e.G0))
-                    jl = min(jl, cyc - i);
-                s = (s + 1) & mask;
-            }
-        }
-        jl = __shfl_sync(FULL, jl, 0);
-        if (jl != ~0u) best = jl;
+        const int i = find_baby_index(f, tbl, B32, 1, cyc, f.key(f.canon(G0)));
+        if (i > 0) best = cyc - (u32)i;
     } else {
         const u64 G = (e.jcount - 1 + m - 1) / m;      // giant steps g = 1..G cover j in [1, G*m]
         for (u64 base = 0; base < G; base += 64) {
             const u64 g0 = base + 1 + lane, g1 = base + 33 + lane;
-            u32 cand = ~0u;
-            if (g0 <= G) cand = min(cand, table_probe(tab, mask, tbits, M.norm(gi0), g0, m, M, e.t, e.B));
-            if (g1 <= G) cand = min(cand, table_probe(tab, mask, tbits, M.norm(gi1), g1, m, M, e.t, e.B));
-            const u32 jmin = __reduce_min_sync(FULL, cand);
+            const u64 k0 = f.key(f.canon(gi0)), k1 = f.key(f.canon(gi1));
+            const bool h0 = g0 <= G && table_maybe(tab, mask, tbits, k0);
+            const bool h1 = g1 <= G && table_maybe(tab, mask, tbits, k1);
+            const u32 bal0 = __ballot_sync(FULL, h0), bal1 = __ballot_sync(FULL, h1);
             steps += min((u64)64, G - base);
-            if (jmin != ~0u) {
-                best = jmin;
-                break;
+            if (bal0 | bal1) {
+                // candidates in increasing g: the first exact one is the smallest j
+                u64 jb = ~0ull;
+                for (int pass = 0; pass < 2 && jb == ~0ull; ++pass) {
+                    u32 bal = pass == 0 ? bal0 : bal1;
+                    while (bal && jb == ~0ull) {
+                        const int src = __ffs(bal) - 1;
+                        bal &= bal - 1;
+                        const u64 kk = __shfl_sync(FULL, pass == 0 ? k0 : k1, src);
+                        const u64 gg = base + (pass == 0 ? 1 : 33) + (u64)src;
+                        const int i = find_baby_index(f, tbl, B32, 0, m, kk);
+                        if (i >= 0) jb = gg * m - (u64)i;
+                    }
+                }
+                if (jb != ~0ull) {
+                    best = jb;
+                    break;
+                }
             }
-            gi0 = M.mul(gi0, Bm64);
-            gi1 = M.mul(gi1, Bm64);
+            gi0 = f.mul(gi0, Bm64);
+            gi1 = f.mul(gi1, Bm64);
         }
     }
     __syncwarp();
@@ -491,10 +768,199 @@ __device__ u64 solve_entry(const Entry& e, u32* tab, u32 tbits, u64* steps_out =
     return best < e.jcount ? best : ~0ull;
 }
 
-__global__ void k_bsgs(BsgsArgs a, Counters* ctr) {
-    extern __shared__ __align__(16) u32 smem[];
+// ---- the FP64 solve (p < 2^49): the hot loop of the whole path ----
+//
+// Table: 2^tbits 32-bit slots per warp.  A key's home slot is the top tbits
+// of a multiplicative hash h of the canonical value's two 32-bit halves; the
+// slot word is (h & ~1) | 2 (never 0) plus bit 0, the overflow bit, set on a
+// home slot when a key homed there had to move further (linear probing).  A
+// probe therefore reads one slot: a match, an empty slot, or an occupied slot
+// without the overflow bit all end it; only an overflowed home (rare at the
+// load factors used) walks the chain, in a ballot-guarded slow path.  A match
+// is resolved exactly by recomputation (ffind_baby): true solutions, and hash
+// collisions at about 2^-20 per compare.
+
+__device__ __forceinline__ u32 fhash(double v) {
+    return (u32)(__double2loint(v) ^ __double2hiint(v)) * 0x9E3779B1u;
+}
+
+__device__ __forceinline__ u32 fword(u32 h) { return (h & ~3u) | 2u; }
+
+__device__ __forceinline__ void ftable_insert(u32* tab, u32 mask, u32 shift, u32 h) {
+    u32 s = h >> shift;
+    const u32 w = fword(h);
+    if (atomicCAS(&tab[s], 0u, w) == 0u) return;
+    atomicOr(&tab[s], 1u);                         // a key homed here moves on
+    do s = (s + 1) & mask;
+    while (atomicCAS(&tab[s], 0u, w) != 0u);
+}
+
+// Continues a probe past an overflowed home slot s.
+__device__ __forceinline__ bool ftable_walk(const u32* tab, u32 mask, u32 s, u32 w) {
+    for (;;) {
+        s = (s + 1) & mask;
+        const u32 e = tab[s];
+        if (e == 0u) return false;
+        if ((e & ~1u) == w) return true;
+    }
+}
+
+// Smallest i in [lo, limit) with t * B^i == v (canonical doubles compared
+// exactly); -1 when there is none.  Warp-cooperative: tbl = t * B^lane.
+__device__ __noinline__ int ffind_baby(const Fp64& f, double tbl, double B32, u32 lo, u32 limit, double v) {
+    const u32 lane = threadIdx.x & 31;
+    double x = tbl;
+    for (u32 base = 0; base < limit; base += 32) {
+        const u32 i = base + lane;
+        const bool hit = i >= lo && i < limit && f.canon(x) == v;
+        const u32 bal = __ballot_sync(FULL, hit);
+        if (bal) return (int)(base + __ffs(bal) - 1);
+        x = f.mul(x, B32);
+    }
+    return -1;
+}
+
+// CH interleaved chains per lane: baby index i = lane + 32c + 32*CH*k,
+// giant step g = 1 + lane + 32c + 32*CH*k.
+template <int CH>
+__device__ u64 solve_fp64(const Entry& e, u32* tab, u32 tbits, u64* steps_out) {
+    const u32 lane = threadIdx.x & 31;
+    Fp64 f;
+    f.init(e.p);
+    const u32 m = e.m;
+    const u32 jc = (u32)e.jcount;                      // jcount <= 10^7
+    const u32 mask = (1u << tbits) - 1, shift = 32 - tbits;
+    const double B = (double)e.B, Bm = (double)e.Bm, tv = (double)e.t, G0 = (double)e.G0;
+
+    double xb = B, xg = Bm;                            // B^(l+1), Bm^(l+1)
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const double yb = __shfl_up_sync(FULL, xb, off), yg = __shfl_up_sync(FULL, xg, off);
+        if (lane >= (u32)off) {
+            xb = f.mul(xb, yb);
+            xg = f.mul(xg, yg);
+        }
+    }
+    const double B32 = __shfl_sync(FULL, xb, 31), Bm32 = __shfl_sync(FULL, xg, 31);
+    double bl = __shfl_up_sync(FULL, xb, 1);
+    if (lane == 0) bl = 1.0;
+    double Bstep = B32, Gstep = Bm32;                  // B^(32 CH), Bm^(32 CH)
+#pragma unroll
+    for (int c = 1; c < CH; c <<= 1) {
+        Bstep = f.mul(Bstep, Bstep);
+        Gstep = f.mul(Gstep, Gstep);
+    }
+    const double tbl = f.mul(tv, bl);
+    double bx[CH], gx[CH];
+    bx[0] = tbl;
+    gx[0] = f.mul(G0, xg);
+#pragma unroll
+    for (int c = 1; c < CH; ++c) {
+        bx[c] = f.mul(bx[c - 1], B32);
+        gx[c] = f.mul(gx[c - 1], Bm32);
+    }
+
+    uint4* t4 = reinterpret_cast<uint4*>(tab);
+    for (u32 k = lane; k <= mask / 4; k += 32) t4[k] = make_uint4(0, 0, 0, 0);
+    __syncwarp();
+
+    // baby steps, stopping at a cycle B^d == 1 (d < m)
+    u32 cyc = 0, baby_done = m;
+    for (u32 base = 0; base < m; base += 32 * CH) {
+        double cv[CH];
+        u32 cb = 0;
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            cv[c] = f.canon(bx[c]);
+            const u32 i = base + 32 * c + lane;
+            const u32 bc = __ballot_sync(FULL, i > 0 && i < m && cv[c] == tv);
+            if (bc && !cb) cb = base + 32 * c + __ffs(bc) - 1;
+        }
+        const u32 lim = cb ? cb : m;
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            const u32 i = base + 32 * c + lane;
+            if (i < lim) ftable_insert(tab, mask, shift, fhash(cv[c]));
+        }
+        if (cb) {
+            cyc = cb;
+            baby_done = cb;
+            break;
+        }
+#pragma unroll
+        for (int c = 0; c < CH; ++c) bx[c] = f.mul(bx[c], Bstep);
+    }
+    __syncwarp();
+
+    u64 best = ~0ull;
+    u32 giant_done = 0;
+    if (cyc) {
+        const int i = ffind_baby(f, tbl, B32, 1, cyc, G0);
+        if (i > 0) best = cyc - (u32)i;
+    } else {
+        const u32 G = (jc - 1 + m - 1) / m;            // g = 1..G covers j in [1, G*m]
+        giant_done = G;
+        for (u32 base = 0; base < G; base += 32 * CH) {
+            double cv[CH];
+            u32 hit = 0;
+#pragma unroll
+            for (int c = 0; c < CH; ++c) {
+                cv[c] = f.canon(gx[c]);
+                const u32 h = fhash(cv[c]);
+                const u32 s0 = h >> shift;
+                const u32 w1 = (h & ~3u) | 3u;         // the slot word with the overflow bit forced
+                const u32 e = tab[s0];
+                bool m1 = (e | 1u) == w1;
+                if (!m1 && (e & 1u)) m1 = ftable_walk(tab, mask, s0, w1 & ~1u);
+                hit |= m1 ? (1u << c) : 0u;
+            }
+            if (__any_sync(FULL, hit)) {
+                u32 bal[CH];
+#pragma unroll
+                for (int c = 0; c < CH; ++c)
+                    bal[c] = __ballot_sync(FULL, ((hit >> c) & 1u) && base + 32 * c + lane + 1 <= G);
+                // candidates in increasing g: the first exact one gives the smallest j
+                u64 jb = ~0ull;
+#pragma unroll
+                for (int c = 0; c < CH; ++c) {
+                    u32 bb = bal[c];
+                    while (bb && jb == ~0ull) {
+                        const int src = __ffs(bb) - 1;
+                        bb &= bb - 1;
+                        const double v = __shfl_sync(FULL, cv[c], src);
+                        const u64 g = base + 32 * c + (u32)src + 1;
+                        const int i = ffind_baby(f, tbl, B32, 0, m, v);
+                        if (i >= 0) jb = g * m - (u64)i;
+                    }
+                }
+                if (jb != ~0ull) {
+                    best = jb;
+                    giant_done = min(G, base + 32 * CH);
+                    break;
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < CH; ++c) gx[c] = f.mul(gx[c], Gstep);
+        }
+    }
+    __syncwarp();
+    if (steps_out) *steps_out = (u64)baby_done + giant_done;
+    return best < e.jcount ? best : ~0ull;
+}
+
+template <int CH>
+__device__ __forceinline__ u64 solve_any(const Entry& e, void* tab, u32 tbits, u64* steps) {
+    if (CH == 0 || e.p >= kFp64Limit) return solve_entry<FieldM>(e, (unsigned short*)tab, tbits + 1, steps);
+    return solve_fp64<CH ? CH : 1>(e, (u32*)tab, tbits, steps);
+}
+
+// CH > 0: every entry has p < 2^49 (FP64 solve with CH chains per lane);
+// CH == 0: any p (integer Montgomery solve).
+template <int CH>
+__global__ void __launch_bounds__(256, MPS_BSGS_MINB) k_bsgs(BsgsArgs a, Counters* ctr) {
+    extern __shared__ __align__(16) u32 smem32[];
     const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    u32* tab = smem + (size_t)warp * (1u << a.tbits);
+    u32* tab = smem32 + (size_t)warp * (1u << a.tbits);
     const u64 n_ent = min((u64)*(volatile unsigned long long*)&ctr->entries, a.ent_cap);
     u64 my_steps = 0;
     if (a.persistent) {
@@ -505,7 +971,7 @@ __global__ void k_bsgs(BsgsArgs a, Counters* ctr) {
             if (idx >= n_ent) break;
             const Entry e = a.ent[idx];
             u64 steps = 0;
-            const u64 j = solve_entry(e, tab, a.tbits, &steps);
+            const u64 j = solve_any<CH>(e, tab, a.tbits, &steps);
             if (lane == 0) {
                 if (j != ~0ull) emit_relation(e.p, e.n_first + j * e.L, 0, e.item, a.rel, a.rel_cap, ctr);
                 my_steps += steps;
@@ -517,7 +983,7 @@ __global__ void k_bsgs(BsgsArgs a, Counters* ctr) {
         if (idx >= n_ent) return;
         const Entry e = a.ent[idx];
         u64 steps = 0;
-        const u64 j = solve_entry(e, tab, a.tbits, &steps);
+        const u64 j = solve_any<CH>(e, tab, a.tbits, &steps);
         if (lane == 0) {
             if (j != ~0ull) emit_relation(e.p, e.n_first + j * e.L, 0, e.item, a.rel, a.rel_cap, ctr);
             atomicAdd(&ctr->steps, (unsigned long long)steps);
@@ -713,19 +1179,13 @@ __global__ void k_is_prime(const u64* n, u32* out, u64 count) {
 
 // cases[5i..5i+4] = p, B, G0, t, jcount (plain residues); one warp per case.
 __global__ void k_bsgs_direct(const u64* cases, u64* j_out, u64 count, u32 tbits) {
-    extern __shared__ __align__(16) u32 smem[];
+    extern __shared__ __align__(16) u32 smem32[];
     const u64 idx = blockIdx.x;
     if (idx >= count) return;
     const u64* c = cases + 5 * idx;
-    Mont M;
-    M.init(c[0]);
-    const u64 rr = M.r2();
+    const u64 p = c[0];
     Entry e;
-    e.p = c[0]; e.ninv = M.ninv; e.one = M.one;
-    e.B = M.to_mont(c[1] % c[0], rr);
-    e.G0 = M.to_mont(c[2] % c[0], rr);
-    e.t = M.to_mont(c[3] % c[0], rr);
-    e.jcount = c[4];
+    e.p = p; e.B = c[1] % p; e.G0 = c[2] % p; e.t = c[3] % p; e.jcount = c[4];
     e.n_first = 0; e.L = 1; e.item = 0;
     u64 result;
     if (e.jcount == 0) {
@@ -739,8 +1199,11 @@ __global__ void k_bsgs_direct(const u64* cases, u64* j_out, u64 count, u32 tbits
         const u32 cap = min(kMaxBaby, (1u << tbits) / 2);
         if (m > cap) m = cap;
         e.m = m;
-        e.Bm = M.pow(e.B, m);
-        result = solve_entry(e, smem, tbits);
+        Mont M;
+        M.init(p);
+        const u64 rr = M.r2();
+        e.Bm = M.from_mont(M.pow(M.to_mont(e.B, rr), m));
+        result = e.p < kFp64Limit ? solve_any<2>(e, smem32, tbits, nullptr) : solve_any<0>(e, smem32, tbits, nullptr);
     }
     if (threadIdx.x == 0) j_out[idx] = result;
 }
@@ -767,16 +1230,22 @@ cudaError_t launch_sieve(const SieveArgs& a, const SieveTables& t, u64* surv, u3
 }
 
 cudaError_t launch_prep(const PrepArgs& a, Counters* ctr, int grid, cudaStream_t s) {
-    k_prep<<<grid, 256, 0, s>>>(a, ctr);
+    k_prep<<<grid, kPrepThreads, 0, s>>>(a, ctr);
     return cudaGetLastError();
 }
 
 cudaError_t launch_bsgs(const BsgsArgs& a, Counters* ctr, int grid, cudaStream_t s) {
     const size_t smem = bsgs_smem_bytes(a.tbits, a.warps_per_block);
-    cudaError_t err = cudaFuncSetAttribute(k_bsgs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (err != cudaSuccess) return err;
-    k_bsgs<<<grid, a.warps_per_block * 32, smem, s>>>(a, ctr);
-    return cudaGetLastError();
+    auto go = [&](auto kern) {
+        cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (err != cudaSuccess) return err;
+        kern<<<grid, a.warps_per_block * 32, smem, s>>>(a, ctr);
+        return cudaGetLastError();
+    };
+    if (a.max_p >= kFp64Limit) return go(k_bsgs<0>);
+    if (a.chains == 4) return go(k_bsgs<4>);
+    if (a.chains == 1) return go(k_bsgs<1>);
+    return go(k_bsgs<2>);
 }
 
 cudaError_t launch_order(const OrderArgs& a, Counters* ctr, int grid, cudaStream_t s) {

@@ -51,7 +51,8 @@ struct BsgsArgs {
     u32 tbits;                 // baby-step table of 2^tbits slots per warp
     u32 warps_per_block;
     u32 persistent;            // 1: work-stealing warps; 0: one warp per entry
-    u64 max_entries;           // non-persistent grid size (entries launched)
+    u32 chains;                // FP64 solve: independent chains per lane (1, 2, 4)
+    u64 max_p;                 // largest p of the entries (>= 2^49: integer solve)
 };
 cudaError_t launch_bsgs(const BsgsArgs& a, Counters* ctr, int grid, cudaStream_t s);
 
