@@ -126,10 +126,11 @@ int mps_batch_relations(mps_ctx* ctx, const mps_item* items, size_t n_items, mps
  * sieved-primes/s metric; not part of the relation path). */
 int mps_count_primes(mps_ctx* ctx, uint64_t lo, uint64_t hi, uint64_t* count);
 
-/* Arithmetic ceilings measured on this device: independent 64-bit Montgomery
- * multiplies per second (the routine every BSGS step runs) and independent
- * 32-bit integer multiply-adds per second (the integer pipe). */
-int mps_measure_peaks(mps_ctx* ctx, double* mmul_per_s, double* imad_per_s);
+/* Arithmetic ceilings measured on this device, from independent chains:
+ * exact FP64-pipe modular multiplies per second (the step of every BSGS
+ * with p < 2^49), 64-bit integer Montgomery multiplies per second (p >=
+ * 2^49), and 32-bit integer multiply-adds per second (the integer pipe). */
+int mps_measure_peaks(mps_ctx* ctx, double* fmul_per_s, double* mmul_per_s, double* imad_per_s);
 
 /* ---- kernel-level hooks for parity tests ---- */
 /* Survivors of the odd sieve of [lo, hi) by the odd primes <= min(65521, sqrt(hi)), ascending. */

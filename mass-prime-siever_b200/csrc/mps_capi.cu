@@ -640,31 +640,32 @@ int mps_count_primes(mps_ctx* c, uint64_t lo, uint64_t hi, uint64_t* count) {
     return MPS_OK;
 }
 
-int mps_measure_peaks(mps_ctx* c, double* mmul_per_s, double* imad_per_s) {
+int mps_measure_peaks(mps_ctx* c, double* fmul_per_s, double* mmul_per_s, double* imad_per_s) {
     if (int r = check_ctx(c)) return r;
     u64* sink = nullptr;
     CK(cudaMalloc((void**)&sink, 64), "alloc");
     const int grid = c->num_sms * 8;
     const u32 iters = 4096;
-    float ms_m = 0, ms_i = 0;
+    float ms[3] = {0, 0, 0};
     cudaError_t e = cudaSuccess;
-    for (int rep = 0; rep < 3 && e == cudaSuccess; ++rep) {     // the last repetition is timed
-        e = cudaEventRecord(c->ev0, c->stream);
-        if (e == cudaSuccess) e = launch_mmul_peak(0x0000F00DF00D1ull, iters, grid, sink, c->stream);
-        if (e == cudaSuccess) e = cudaEventRecord(c->ev1, c->stream);
-        if (e == cudaSuccess) e = cudaEventSynchronize(c->ev1);
-        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms_m, c->ev0, c->ev1);
-        if (e == cudaSuccess) e = cudaEventRecord(c->ev0, c->stream);
-        if (e == cudaSuccess) e = launch_imad_peak(iters * 8, grid, (u32*)sink, c->stream);
-        if (e == cudaSuccess) e = cudaEventRecord(c->ev1, c->stream);
-        if (e == cudaSuccess) e = cudaEventSynchronize(c->ev1);
-        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms_i, c->ev0, c->ev1);
+    for (int rep = 0; rep < 2 && e == cudaSuccess; ++rep) {     // the second repetition is kept
+        for (int k = 0; k < 3 && e == cudaSuccess; ++k) {
+            e = cudaEventRecord(c->ev0, c->stream);
+            if (e != cudaSuccess) break;
+            if (k == 0) e = launch_fmul_peak(0x00005639F00D1ull, iters, grid, sink, c->stream);
+            if (k == 1) e = launch_mmul_peak(0x00005639F00D1ull, iters, grid, sink, c->stream);
+            if (k == 2) e = launch_imad_peak(iters * 8, grid, (u32*)sink, c->stream);
+            if (e == cudaSuccess) e = cudaEventRecord(c->ev1, c->stream);
+            if (e == cudaSuccess) e = cudaEventSynchronize(c->ev1);
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms[k], c->ev0, c->ev1);
+        }
     }
     cudaFree(sink);
     if (e != cudaSuccess) return cuda_fail(c, e, "peak probes");
-    const double threads = (double)grid * 256.0;
-    if (mmul_per_s) *mmul_per_s = threads * 8.0 * iters / (ms_m * 1e-3);
-    if (imad_per_s) *imad_per_s = threads * 8.0 * iters * 8.0 / (ms_i * 1e-3);
+    const double ops = (double)grid * 256.0 * 8.0 * iters;
+    if (fmul_per_s) *fmul_per_s = ops / (ms[0] * 1e-3);
+    if (mmul_per_s) *mmul_per_s = ops / (ms[1] * 1e-3);
+    if (imad_per_s) *imad_per_s = ops * 8.0 / (ms[2] * 1e-3);
     return MPS_OK;
 }
 

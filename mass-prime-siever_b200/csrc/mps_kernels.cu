@@ -1034,10 +1034,31 @@ __device__ u64 rho_factor(u64 n) {
     return 0;
 }
 
-// q = ord_p(b), b mod p != 0, p prime (Math.hpp:294-310): factor p - 1 by
-// the sieving primes (divisibility by multiplicative inverses), finish the
-// cofactor by Miller-Rabin / Pollard rho, then strip each prime factor.
-__device__ u64 mult_order(u64 b, u64 p, const SieveTables& t, bool* failed) {
+// Exact 12-base Miller-Rabin (Math.hpp:209-251) with the bases spread over
+// the lanes of a warp: lane k < 12 tries base k.  Warp-uniform result.
+__device__ bool warp_is_prime64(u64 n) {
+    const u32 lane = threadIdx.x & 31;
+    const u32 bases[12] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37};
+    if (n < 2) return false;
+    for (int i = 0; i < 12; ++i) {
+        if (n == bases[i]) return true;
+        if (n % bases[i] == 0) return false;
+    }
+    bool ok = true;
+    if (lane < 12) {
+        Mont M;
+        M.init(n);
+        ok = sprp(M, bases[lane], M.r2());
+    }
+    return __all_sync(FULL, ok);
+}
+
+// q = ord_p(b), b mod p != 0, p prime (Math.hpp:294-310), one warp: the
+// lanes split the trial division of p - 1 by the sieving primes (divisibility
+// by multiplicative inverses); the cofactor is finished by Miller-Rabin /
+// Pollard rho; then each prime factor is stripped from the order.
+__device__ u64 warp_mult_order(u64 b, u64 p, const SieveTables& t, bool* failed) {
+    const u32 lane = threadIdx.x & 31;
     if (p < 1000) {
         u64 x = b % p, k = 1;
         while (x != 1) {
@@ -1048,33 +1069,43 @@ __device__ u64 mult_order(u64 b, u64 p, const SieveTables& t, bool* failed) {
     }
     u64 f[24];
     int nf = 0;
-    u64 n = p - 1;
-    const int tz = __ffsll((long long)n) - 1;
-    n >>= tz;
+    const u64 pm1 = p - 1;
+    const u64 n0 = pm1 >> (__ffsll((long long)pm1) - 1);    // odd part
     f[nf++] = 2;
-    for (u32 k = 0; k < kSievePrimes; ++k) {
-        const u64 q = t.sp[k];
-        if (q * q > n) break;
-        const u64 qi = t.inv[k], lim = t.rcp[k];
-        if (n * qi <= lim) {
-            f[nf++] = q;
-            do n *= qi; while (n * qi <= lim);
+    for (u32 base = 0; base < kSievePrimes; base += 32) {
+        const u32 k = base + lane;
+        const u64 q = k < kSievePrimes ? t.sp[k] : 0;
+        const bool live = k < kSievePrimes && q * q <= n0;
+        const bool div = live && n0 * t.inv[k] <= t.rcp[k];
+        u32 bal = __ballot_sync(FULL, div);
+        while (bal) {
+            const int src = __ffs(bal) - 1;
+            bal &= bal - 1;
+            const u64 qf = __shfl_sync(FULL, q, src);
+            if (nf < 24) f[nf++] = qf;
         }
+        if (!__any_sync(FULL, live)) break;
     }
-    if (n > 1) {
+    // the cofactor of n0 by the small factors found
+    u64 c = n0;
+    for (int i = 1; i < nf; ++i)
+        while (c % f[i] == 0) c /= f[i];
+    if (c > 1) {
         u64 stack[8];
         int sp = 0;
-        stack[sp++] = n;
+        stack[sp++] = c;
         while (sp > 0) {
             const u64 x = stack[--sp];
             if (x == 1) continue;
-            if ((x < (u64)kSieveMaxPrime * kSieveMaxPrime) || is_prime64(x)) {
+            if (x < (u64)kSieveMaxPrime * kSieveMaxPrime || warp_is_prime64(x)) {
                 bool dup = false;
                 for (int i = 0; i < nf; ++i) dup |= f[i] == x;
                 if (!dup && nf < 24) f[nf++] = x;
                 continue;
             }
-            const u64 dv = rho_factor(x);
+            u64 dv = 0;
+            if (lane == 0) dv = rho_factor(x);
+            dv = __shfl_sync(FULL, dv, 0);
             if (dv == 0 || sp + 2 > 8) {
                 *failed = true;
                 return 0;
@@ -1086,27 +1117,32 @@ __device__ u64 mult_order(u64 b, u64 p, const SieveTables& t, bool* failed) {
     Mont M;
     M.init(p);
     const u64 bm = M.to_mont(b % p, M.r2());
-    u64 order = p - 1;
+    u64 order = pm1;
     for (int i = 0; i < nf; ++i) {
         while (order % f[i] == 0 && M.pow(bm, order / f[i]) == M.one) order /= f[i];
     }
     return order;
 }
 
+// One warp per relation: exact primality of p (composite survivors are
+// dropped, q = ~0) and q = ord_p(b).
 __global__ void __launch_bounds__(128) k_order(OrderArgs a, Counters* ctr) {
     const u64 n = min((u64)*(volatile unsigned long long*)&ctr->relations, a.rel_cap);
-    for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+    const u32 lane = threadIdx.x & 31;
+    const u64 w0 = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
+    const u64 nw = ((u64)gridDim.x * blockDim.x) >> 5;
+    for (u64 i = w0; i < n; i += nw) {
         RawRelation r = a.rel[i];
-        if (!is_prime64(r.p)) {
-            r.q = ~0ull;                                // a composite survivor: dropped
+        if (!warp_is_prime64(r.p)) {
+            r.q = ~0ull;
         } else if (r.q == 0) {
             const DevItem& it = a.items[r.item];
             const u64 b_mod = residue128(it.babs_hi, it.babs_lo, it.b_neg, r.p);
             bool failed = false;
-            r.q = mult_order(b_mod, r.p, a.tables, &failed);
-            if (failed) atomicOr(&ctr->status, kStatusOrderFailed);
+            r.q = warp_mult_order(b_mod, r.p, a.tables, &failed);
+            if (failed && lane == 0) atomicOr(&ctr->status, kStatusOrderFailed);
         }
-        a.rel[i] = r;
+        if (lane == 0) a.rel[i] = r;
     }
 }
 
@@ -1152,6 +1188,24 @@ __global__ void __launch_bounds__(256) k_mmul_peak(u64 p0, u32 iters, u64* sink)
 #pragma unroll
     for (int k = 0; k < 8; ++k) acc ^= x[k];
     if (acc == 0x123456789ull) sink[0] = acc;
+}
+
+// Independent exact FP64 modular multiplies (p < 2^49): 8 chains per thread.
+__global__ void __launch_bounds__(256) k_fmul_peak(u64 p0, u32 iters, u64* sink) {
+    Fp64 f;
+    f.init(p0 | 1);
+    double x[8];
+    const double y = (double)((0x9E3779B97F4A7C15ull ^ threadIdx.x) % f.pi);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = (double)((blockIdx.x * 8191ull + threadIdx.x * 31ull + k) % f.pi);
+    for (u32 i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) x[k] = f.mul(x[k], y);
+    }
+    double acc = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) acc += x[k];
+    if (acc == 123.0) sink[0] = (u64)acc;
 }
 
 // Independent 32-bit multiply-adds: 8 chains per thread.
@@ -1209,10 +1263,12 @@ __global__ void k_bsgs_direct(const u64* cases, u64* j_out, u64 count, u32 tbits
 }
 
 __global__ void k_order_direct(const u64* bp, u64* q_out, u64 count, SieveTables t) {
-    for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < count; i += (u64)gridDim.x * blockDim.x) {
+    const u64 w0 = (blockIdx.x * (u64)blockDim.x + threadIdx.x) >> 5;
+    const u64 nw = ((u64)gridDim.x * blockDim.x) >> 5;
+    for (u64 i = w0; i < count; i += nw) {
         bool failed = false;
-        const u64 q = mult_order(bp[2 * i], bp[2 * i + 1], t, &failed);
-        q_out[i] = failed ? 0 : q;
+        const u64 q = warp_mult_order(bp[2 * i], bp[2 * i + 1], t, &failed);
+        if ((threadIdx.x & 31) == 0) q_out[i] = failed ? 0 : q;
     }
 }
 
@@ -1263,6 +1319,11 @@ cudaError_t launch_mmul_peak(u64 p, u32 iters, int grid, u64* sink, cudaStream_t
     return cudaGetLastError();
 }
 
+cudaError_t launch_fmul_peak(u64 p, u32 iters, int grid, u64* sink, cudaStream_t s) {
+    k_fmul_peak<<<grid, 256, 0, s>>>(p, iters, sink);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_imad_peak(u32 iters, int grid, u32* sink, cudaStream_t s) {
     k_imad_peak<<<grid, 256, 0, s>>>(iters, sink);
     return cudaGetLastError();
@@ -1285,7 +1346,7 @@ cudaError_t launch_bsgs_direct(const u64* cases, u64* j_out, u64 count, u32 tbit
 
 cudaError_t launch_order_direct(const u64* bp, u64* q_out, u64 count, SieveTables t, cudaStream_t s) {
     if (count == 0) return cudaSuccess;
-    k_order_direct<<<(unsigned)min((count + 63) / 64, (u64)4096), 64, 0, s>>>(bp, q_out, count, t);
+    k_order_direct<<<(unsigned)min((count + 3) / 4, (u64)4096), 128, 0, s>>>(bp, q_out, count, t);
     return cudaGetLastError();
 }
 

@@ -71,6 +71,7 @@ cudaError_t launch_count_primes(const u64* surv, u64 surv_cap, Counters* ctr, in
 // Roofline probes: 256 x grid threads x 8 independent chains x iters operations.
 cudaError_t launch_mmul_peak(u64 p, u32 iters, int grid, u64* sink, cudaStream_t s);
 cudaError_t launch_imad_peak(u32 iters, int grid, u32* sink, cudaStream_t s);
+cudaError_t launch_fmul_peak(u64 p, u32 iters, int grid, u64* sink, cudaStream_t s);
 
 // Test hooks: raw kernels on given inputs.
 cudaError_t launch_is_prime(const u64* n, u32* out, u64 count, cudaStream_t s);

@@ -102,7 +102,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.mps_filter.argtypes = [vp, P(u64), sz, P(Item), P(ctypes.c_uint8)]
     L.mps_batch_relations.argtypes = [vp, P(Item), sz, P(Relation), P(u32), sz, P(sz)]
     L.mps_count_primes.argtypes = [vp, u64, u64, P(u64)]
-    L.mps_measure_peaks.argtypes = [vp, P(ctypes.c_double), P(ctypes.c_double)]
+    L.mps_measure_peaks.argtypes = [vp, P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_double)]
     L.mps_test_survivors.argtypes = [vp, u64, u64, P(u64), sz, P(sz)]
     L.mps_test_is_prime.argtypes = [vp, P(u64), sz, P(ctypes.c_uint8)]
     L.mps_test_bsgs.argtypes = [vp, P(u64), sz, u32, P(u64)]
@@ -221,10 +221,10 @@ class Siever:
         self._check(self.lib.mps_count_primes(self.ctx, lo, hi, ctypes.byref(c)))
         return c.value
 
-    def measure_peaks(self) -> tuple[float, float]:
-        a, b = ctypes.c_double(), ctypes.c_double()
-        self._check(self.lib.mps_measure_peaks(self.ctx, ctypes.byref(a), ctypes.byref(b)))
-        return a.value, b.value
+    def measure_peaks(self) -> dict:
+        a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.mps_measure_peaks(self.ctx, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return {"fp64_mulmod_per_s": a.value, "int_mulmod_per_s": b.value, "imad_per_s": c.value}
 
     def survivors(self, lo: int, hi: int, cap: int = 1 << 16) -> list[int]:
         while True:
