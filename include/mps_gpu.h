@@ -132,6 +132,20 @@ int mps_count_primes(mps_ctx* ctx, uint64_t lo, uint64_t hi, uint64_t* count);
  * 2^49), and 32-bit integer multiply-adds per second (the integer pipe). */
 int mps_measure_peaks(mps_ctx* ctx, double* fmul_per_s, double* mmul_per_s, double* imad_per_s);
 
+/* ---- relations of one small range without allocating (no counterpart in the reference) ----
+ * For callers that cannot allocate device memory where they sieve: their
+ * device memory belongs to another framework's pool allocator, or cudaMalloc
+ * / cudaFree (which synchronise the device) are not allowed in their loop.
+ * Same result as mps_chunk_relations with the default tuning, on the calling
+ * thread's current device and the default stream, with no context.  All
+ * scratch is one static device array of 8 MiB that every GPU loading this
+ * library holds until exit; its address is looked up on the first call on
+ * each device (make that first call before any stream capture).  Calls share
+ * that array, so calls that overlap on the GPU race and must not be made.
+ * hi - lo must not exceed 2^19 (MPS_E_RANGE otherwise); hi <= 2^62. */
+int mps_chunk_relations_noalloc(uint64_t lo, uint64_t hi, const mps_item* item,
+                                mps_relation* out, size_t cap, size_t* n_out);
+
 /* ---- kernel-level hooks for parity tests ---- */
 /* Survivors of the odd sieve of [lo, hi) by the odd primes <= min(65521, sqrt(hi)), ascending. */
 int mps_test_survivors(mps_ctx* ctx, uint64_t lo, uint64_t hi, uint64_t* out, size_t cap, size_t* n_out);
