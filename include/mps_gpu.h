@@ -122,6 +122,12 @@ int mps_filter(mps_ctx* ctx, const uint64_t* primes, size_t n, const mps_item* i
 int mps_batch_relations(mps_ctx* ctx, const mps_item* items, size_t n_items, mps_relation* out,
                         uint32_t* out_item, size_t cap, size_t* n_out);
 
+/* The relations of the last mps_chunk_relations / mps_item_relations /
+ * mps_batch_relations call again, without recomputing them: after such a call
+ * returned MPS_E_CAPACITY (with *n_out = the count), pass a buffer of that
+ * size here.  out_item may be NULL. */
+int mps_take_relations(mps_ctx* ctx, mps_relation* out, uint32_t* out_item, size_t cap, size_t* n_out);
+
 /* Number of primes in [lo, hi) counted on the device (the unit of the
  * sieved-primes/s metric; not part of the relation path). */
 int mps_count_primes(mps_ctx* ctx, uint64_t lo, uint64_t hi, uint64_t* count);

@@ -58,6 +58,30 @@ u64 gcd_u64(u64 a, u64 b) {
 
 }  // namespace
 
+// One of the two in-flight wave slots of the batched engine.
+struct WaveSlot {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_b0 = nullptr, ev_b1 = nullptr;
+    u64* d_surv = nullptr;
+    u32* d_surv_item = nullptr;
+    u64 surv_cap = 0;
+    Entry* d_ent = nullptr;
+    u64 ent_cap = 0;
+    RawRelation* d_rel = nullptr;
+    RawRelation* h_rel = nullptr;     // pinned
+    u64 rel_cap = 0;
+    Counters* d_ctr = nullptr;
+    Counters* h_ctr = nullptr;        // pinned
+    WaveDesc* d_wave = nullptr;
+    WaveDesc* h_wave = nullptr;       // pinned
+    cudaGraphExec_t graph = nullptr;
+    u32 graph_tbits = 0;
+    const DevItem* graph_items = nullptr;
+    bool busy = false;
+    std::vector<std::pair<u64, u64>> ranges;   // (lo, hi) of each run in flight
+    std::vector<u32> range_item;
+};
+
 struct mps_ctx {
     int device = 0;
     int num_sms = 148;
@@ -84,6 +108,10 @@ struct mps_ctx {
     u64 rel_cap = 0;
     DevItem* d_items = nullptr;
     u64 items_cap = 0;
+    WaveSlot slot[2];
+    bool slots_ready = false;
+    std::vector<u64> item_K;           // K of each item on the device (table sizing)
+    std::vector<RawRelation> last;     // relations of the last call (kept for mps_take_relations)
 
     SieveTables tables() const { return SieveTables{d_sp, d_rcp, d_inv}; }
 };
@@ -348,6 +376,236 @@ int run_chunk(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, std::vector<RawRelati
     return MPS_OK;
 }
 
+
+// ------------------------------------------------------------ the wave engine --
+//
+// Items are cut into pieces of at most chunk_odds odd numbers; pieces are
+// packed into waves of at most chunk_odds odd numbers in total (up to
+// kMaxRuns runs, possibly of different items).  A wave runs as
+//   H2D wave descriptor -> counters reset -> k_sieve_wave -> k_prep -> k_bsgs
+//   -> k_order -> D2H counters + first relations
+// on one of two slots (own stream and buffers), captured once per slot as a
+// CUDA graph and replayed for every wave.  While the host reads wave k's
+// results the device already runs wave k+1 on the other slot, so the tail of
+// one wave's BSGS overlaps the next wave's sieve and prep.
+
+constexpr u64 kGraphRelations = 4096;    // relations copied back inside the graph
+
+int slot_alloc(mps_ctx* c, WaveSlot& w) {
+    const u64 chunk = c->tun.chunk_odds;
+    if (!w.stream) {
+        CK(cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking), "stream");
+        CK(cudaEventCreate(&w.ev_b0), "event");
+        CK(cudaEventCreate(&w.ev_b1), "event");
+        CK(cudaMalloc((void**)&w.d_ctr, sizeof(Counters)), "counters");
+        CK(cudaMallocHost((void**)&w.h_ctr, sizeof(Counters)), "counters");
+        CK(cudaMalloc((void**)&w.d_wave, sizeof(WaveDesc)), "wave descriptor");
+        CK(cudaMallocHost((void**)&w.h_wave, sizeof(WaveDesc)), "wave descriptor");
+    }
+    if (w.surv_cap < chunk + kMaxRuns + 16) {
+        if (w.d_surv) CK(cudaFree(w.d_surv), "cudaFree");
+        if (w.d_surv_item) CK(cudaFree(w.d_surv_item), "cudaFree");
+        w.surv_cap = chunk + kMaxRuns + 16;
+        CK(cudaMalloc((void**)&w.d_surv, w.surv_cap * sizeof(u64)), "survivor buffer");
+        CK(cudaMalloc((void**)&w.d_surv_item, w.surv_cap * sizeof(u32)), "survivor items");
+        if (w.graph) cudaGraphExecDestroy(w.graph);
+        w.graph = nullptr;
+    }
+    if (w.ent_cap < std::max<u64>(chunk / 4, 1 << 16)) {
+        if (w.d_ent) CK(cudaFree(w.d_ent), "cudaFree");
+        w.ent_cap = std::max<u64>(chunk / 4, 1 << 16);
+        CK(cudaMalloc((void**)&w.d_ent, w.ent_cap * sizeof(Entry)), "entry buffer");
+        if (w.graph) cudaGraphExecDestroy(w.graph);
+        w.graph = nullptr;
+    }
+    if (w.rel_cap < (1u << 16)) {
+        w.rel_cap = 1u << 16;
+        CK(cudaMalloc((void**)&w.d_rel, w.rel_cap * sizeof(RawRelation)), "relation buffer");
+        CK(cudaMallocHost((void**)&w.h_rel, w.rel_cap * sizeof(RawRelation)), "relation buffer");
+    }
+    return MPS_OK;
+}
+
+void slot_free(WaveSlot& w) {
+    if (w.stream) cudaStreamSynchronize(w.stream);
+    if (w.graph) cudaGraphExecDestroy(w.graph);
+    for (void* p : {(void*)w.d_surv, (void*)w.d_surv_item, (void*)w.d_ent, (void*)w.d_rel, (void*)w.d_ctr,
+                    (void*)w.d_wave})
+        if (p) cudaFree(p);
+    for (void* p : {(void*)w.h_rel, (void*)w.h_ctr, (void*)w.h_wave})
+        if (p) cudaFreeHost(p);
+    if (w.ev_b0) cudaEventDestroy(w.ev_b0);
+    if (w.ev_b1) cudaEventDestroy(w.ev_b1);
+    if (w.stream) cudaStreamDestroy(w.stream);
+    w = WaveSlot();
+}
+
+// The per-wave launch sequence on the slot's stream (captured or direct).
+int slot_enqueue(mps_ctx* c, WaveSlot& w, u32 tbits, bool capturing) {
+    const cudaStream_t s = w.stream;
+    const u32 warps = c->tun.bsgs_warps;
+    PrepArgs pa{};
+    pa.surv = w.d_surv; pa.surv_cap = w.surv_cap; pa.surv_item = w.d_surv_item; pa.item0 = 0;
+    pa.items = c->d_items; pa.ent = w.d_ent; pa.ent_cap = w.ent_cap; pa.rel = w.d_rel; pa.rel_cap = w.rel_cap;
+    pa.full_mr = c->tun.full_mr;
+    BsgsArgs ba{};
+    ba.ent = w.d_ent; ba.ent_cap = w.ent_cap; ba.rel = w.d_rel; ba.rel_cap = w.rel_cap; ba.tbits = tbits;
+    ba.warps_per_block = warps; ba.persistent = 1; ba.chains = c->tun.reserved[0] ? c->tun.reserved[0] : 2;
+    ba.max_p = 0;   // per-entry arithmetic
+    OrderArgs oa{};
+    oa.rel = w.d_rel; oa.rel_cap = w.rel_cap; oa.items = c->d_items; oa.tables = c->tables();
+    int bgrid = 0;
+    if (int r = bsgs_grid(c, tbits, warps, &bgrid)) return r;
+    CK(cudaMemcpyAsync(w.d_wave, w.h_wave, sizeof(WaveDesc), cudaMemcpyHostToDevice, s), "wave upload");
+    CK(cudaMemsetAsync(w.d_ctr, 0, sizeof(Counters), s), "counter reset");
+    CK(launch_sieve_wave(w.d_wave, c->tables(), w.d_surv, w.d_surv_item, w.surv_cap, w.d_ctr, grid_for(c, 8), s),
+       "sieve launch");
+    CK(launch_prep(pa, w.d_ctr, grid_for(c, 16), s), "prep launch");
+    // external records: a captured graph records these events on every replay
+    const unsigned ev_flags = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+    CK(cudaEventRecordWithFlags(w.ev_b0, s, ev_flags), "event");
+    CK(launch_bsgs(ba, w.d_ctr, bgrid, s), "bsgs launch");
+    CK(cudaEventRecordWithFlags(w.ev_b1, s, ev_flags), "event");
+    CK(launch_order(oa, w.d_ctr, grid_for(c, 4), s), "order launch");
+    CK(cudaMemcpyAsync(w.h_ctr, w.d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, s), "count read");
+    CK(cudaMemcpyAsync(w.h_rel, w.d_rel, kGraphRelations * sizeof(RawRelation), cudaMemcpyDeviceToHost, s),
+       "relation read");
+    return MPS_OK;
+}
+
+int slot_launch(mps_ctx* c, WaveSlot& w, u32 tbits) {
+    if (c->tun.reserved[1]) return slot_enqueue(c, w, tbits, false);       // graphs off (tuning)
+    if (!w.graph || w.graph_tbits != tbits || w.graph_items != c->d_items) {
+        if (w.graph) cudaGraphExecDestroy(w.graph);
+        w.graph = nullptr;
+        CK(bsgs_reserve_smem(bsgs_smem_bytes(tbits, c->tun.bsgs_warps)), "bsgs shared memory");
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(w.stream, cudaStreamCaptureModeThreadLocal), "capture");
+        const int r = slot_enqueue(c, w, tbits, true);
+        cudaError_t e = cudaStreamEndCapture(w.stream, &g);
+        if (r) {
+            if (g) cudaGraphDestroy(g);
+            return r;
+        }
+        if (e != cudaSuccess) return cuda_fail(c, e, "end capture");
+        e = cudaGraphInstantiate(&w.graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return cuda_fail(c, e, "graph instantiate");
+        w.graph_tbits = tbits;
+        w.graph_items = c->d_items;
+    }
+    CK(cudaGraphLaunch(w.graph, w.stream), "graph launch");
+    return MPS_OK;
+}
+
+// Waits for the slot's wave and appends its relations; on a buffer overflow
+// the wave's runs are redone one by one on the chunk path (which splits them).
+int slot_finish(mps_ctx* c, WaveSlot& w, std::vector<RawRelation>& out) {
+    if (!w.busy) return MPS_OK;
+    w.busy = false;
+    CK(cudaStreamSynchronize(w.stream), "wave");
+    const Counters h = *w.h_ctr;
+    float bms = 0;
+    CK(cudaEventElapsedTime(&bms, w.ev_b0, w.ev_b1), "event time");
+    c->stats.bsgs_ms += bms;
+    c->stats.bsgs_launches += 1;
+    c->stats.kernel_launches += 4;
+    if (h.status & kStatusOrderFailed) return fail(c, MPS_E_CUDA, "order computation did not factor p - 1");
+    if (h.status & (kStatusSurvivorOverflow | kStatusEntryOverflow | kStatusRelationOverflow)) {
+        for (size_t i = 0; i < w.ranges.size(); ++i) {
+            std::vector<RawRelation> part;
+            const DevItem* items = c->d_items;
+            (void)items;
+            if (int r = run_chunk(c, w.ranges[i].first, w.ranges[i].second, w.range_item[i],
+                                  c->item_K[w.range_item[i]], part))
+                return r;
+            out.insert(out.end(), part.begin(), part.end());
+        }
+        return MPS_OK;
+    }
+    const u64 nr = h.relations;
+    if (nr > kGraphRelations)
+        CK(cudaMemcpy(w.h_rel + kGraphRelations, w.d_rel + kGraphRelations,
+                      (nr - kGraphRelations) * sizeof(RawRelation), cudaMemcpyDeviceToHost),
+           "relation read");
+    for (u64 i = 0; i < nr; ++i)
+        if (w.h_rel[i].q != ~0ull) out.push_back(w.h_rel[i]);
+    c->stats.bsgs_steps += h.steps;
+    c->stats.survivors += h.survivors;
+    c->stats.entries += h.entries;
+    c->stats.chunks += 1;
+    return MPS_OK;
+}
+
+// Relations of the items already on the device (d_items, item_K set), each
+// over [lo_i, hi_i), through the double-buffered wave engine.
+int run_waves(mps_ctx* c, const std::vector<u64>& lo, const std::vector<u64>& hi, std::vector<RawRelation>& out) {
+    if (!c->slots_ready) {
+        for (WaveSlot& w : c->slot)
+            if (int r = slot_alloc(c, w)) return r;
+        c->slots_ready = true;
+    }
+    for (WaveSlot& w : c->slot)
+        if (int r = slot_alloc(c, w)) return r;
+    u32 tbits = 5;
+    for (size_t i = 0; i < lo.size(); ++i) {
+        u32 tb, mb;
+        table_for(c, c->item_K[i], &tb, &mb);
+        tbits = std::max(tbits, tb);
+    }
+    const u64 chunk = c->tun.chunk_odds;
+    int k = 0;
+    WaveSlot* cur = nullptr;
+    u64 wave_odds = 0;
+    auto flush = [&]() -> int {
+        if (!cur || cur->h_wave->n_runs == 0) return MPS_OK;
+        cur->h_wave->total_segs = 0;
+        for (u32 r = 0; r < cur->h_wave->n_runs; ++r) {
+            cur->h_wave->runs[r].seg_begin = cur->h_wave->total_segs;
+            cur->h_wave->total_segs += (cur->h_wave->runs[r].n_odds + kSieveSegOdds - 1) / kSieveSegOdds;
+        }
+        if (int r = slot_launch(c, *cur, tbits)) return r;
+        cur->busy = true;
+        k ^= 1;
+        cur = nullptr;
+        wave_odds = 0;
+        return MPS_OK;
+    };
+    for (size_t i = 0; i < lo.size(); ++i) {
+        for (u64 a = lo[i]; a < hi[i];) {
+            const u64 lo_odd = std::max<u64>(a, 3) | 1ull;
+            if (!cur) {
+                cur = &c->slot[k];
+                if (int r = slot_finish(c, *cur, out)) return r;   // the slot's previous wave
+                cur->h_wave->n_runs = 0;
+                cur->ranges.clear();
+                cur->range_item.clear();
+            }
+            const u64 room = chunk - wave_odds;
+            u64 b = hi[i];
+            if (lo_odd < hi[i] && (hi[i] - lo_odd + 1) / 2 > room) b = lo_odd + 2 * room;
+            SieveRun& run = cur->h_wave->runs[cur->h_wave->n_runs++];
+            run.lo_odd = lo_odd;
+            run.n_odds = lo_odd < b ? (b - lo_odd + 1) / 2 : 0;
+            run.include_two = (a <= 2 && b > 2) ? 1 : 0;
+            run.n_primes = sieve_prime_count(b);
+            run.item = (u32)i;
+            run.pad = 0;
+            cur->ranges.push_back({a, b});
+            cur->range_item.push_back((u32)i);
+            wave_odds += run.n_odds;
+            c->stats.odds += run.n_odds;
+            a = b;
+            if (wave_odds >= chunk || cur->h_wave->n_runs == kMaxRuns)
+                if (int r = flush()) return r;
+        }
+    }
+    if (int r = flush()) return r;
+    for (int j = 0; j < 2; ++j)
+        if (int r = slot_finish(c, c->slot[(k + j) & 1], out)) return r;
+    return MPS_OK;
+}
+
 int check_ctx(mps_ctx* c) {
     if (!c) return MPS_E_ARG;
     if (c->poisoned) return fail(c, MPS_E_STATE, "context poisoned by an earlier device fault: " + c->err);
@@ -402,7 +660,8 @@ int copy_out(mps_ctx* c, const std::vector<RawRelation>& rel, mps_relation* out,
              size_t* n_out) {
     if (n_out) *n_out = rel.size();
     c->stats.relations = rel.size();
-    if (rel.size() > cap) return fail(c, MPS_E_CAPACITY, "output buffer too small");
+    if (&rel != &c->last) c->last = rel;
+    if (rel.size() > cap) return fail(c, MPS_E_CAPACITY, "output buffer too small (mps_take_relations returns them)");
     for (size_t i = 0; i < rel.size(); ++i) {
         out[i].p = rel[i].p;
         out[i].M = rel[i].M;
@@ -480,6 +739,7 @@ int mps_close(mps_ctx* c) {
     if (!c) return MPS_E_ARG;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    for (WaveSlot& w : c->slot) slot_free(w);
     for (void* p : {(void*)c->d_sp, (void*)c->d_rcp, (void*)c->d_inv, (void*)c->d_ctr, (void*)c->d_surv,
                     (void*)c->d_surv_item, (void*)c->d_ent, (void*)c->d_rel, (void*)c->d_items})
         if (p) cudaFree(p);
@@ -514,7 +774,18 @@ int mps_chunk_relations(mps_ctx* c, uint64_t lo, uint64_t hi, const mps_item* it
 
 int mps_item_relations(mps_ctx* c, const mps_item* item, mps_relation* out, size_t cap, size_t* n_out) {
     if (!item) return fail(c, MPS_E_ARG, "item is NULL");
-    return mps_chunk_relations(c, item->P0, item->P1, item, out, cap, n_out);
+    if (c && c->tun.plain) return mps_chunk_relations(c, item->P0, item->P1, item, out, cap, n_out);
+    if (int r = check_ctx(c)) return r;
+    DevItem d;
+    if (int r = make_dev_item(c, item, 0, &d)) return r;
+    begin_call(c);
+    std::vector<RawRelation> rel;
+    c->item_K.assign(1, d.K);
+    if (int r = upload_items(c, &d, 1)) return r;
+    if (int r = run_waves(c, {item->P0}, {item->P1}, rel)) return r;
+    if (int r = end_call(c)) return r;
+    sort_by_p(rel);
+    return copy_out(c, rel, out, nullptr, cap, n_out);
 }
 
 int mps_sieve_filter(mps_ctx* c, uint64_t lo, uint64_t hi, const mps_item* item, uint64_t* out, size_t cap,
@@ -600,17 +871,35 @@ int mps_batch_relations(mps_ctx* c, const mps_item* items, size_t n_items, mps_r
                         size_t cap, size_t* n_out) {
     if (int r = check_ctx(c)) return r;
     if (!items && n_items) return fail(c, MPS_E_ARG, "items is NULL");
-    begin_call(c);
-    std::vector<RawRelation> rel;
     std::vector<DevItem> d(n_items);
     for (size_t i = 0; i < n_items; ++i)
         if (int r = make_dev_item(c, &items[i], (u32)i, &d[i])) return r;
+    begin_call(c);
+    std::vector<RawRelation> rel;
+    c->item_K.assign(n_items, 0);
+    for (size_t i = 0; i < n_items; ++i) c->item_K[i] = d[i].K;
     if (int r = upload_items(c, d.data(), n_items)) return r;
-    for (size_t i = 0; i < n_items; ++i)
-        if (int r = run_range(c, items[i].P0, items[i].P1, (u32)i, d[i].K, rel)) return r;
+    if (c->tun.plain) {
+        // the plain path: one item after another, one chunk at a time
+        for (size_t i = 0; i < n_items; ++i)
+            if (int r = run_range(c, items[i].P0, items[i].P1, (u32)i, d[i].K, rel)) return r;
+    } else {
+        std::vector<u64> lo(n_items), hi(n_items);
+        for (size_t i = 0; i < n_items; ++i) {
+            lo[i] = items[i].P0;
+            hi[i] = items[i].P1;
+        }
+        if (int r = run_waves(c, lo, hi, rel)) return r;
+    }
     if (int r = end_call(c)) return r;
     sort_by_p(rel);
     return copy_out(c, rel, out, out_item, cap, n_out);
+}
+
+int mps_take_relations(mps_ctx* c, mps_relation* out, uint32_t* out_item, size_t cap, size_t* n_out) {
+    if (!c) return MPS_E_ARG;
+    if (!out && cap) return fail(c, MPS_E_ARG, "out is NULL");
+    return copy_out(c, c->last, out, out_item, cap, n_out);
 }
 
 int mps_count_primes(mps_ctx* c, uint64_t lo, uint64_t hi, uint64_t* count) {

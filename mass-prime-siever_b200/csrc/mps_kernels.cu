@@ -92,134 +92,169 @@ __device__ __forceinline__ u64 first_strike(u64 v0, u32 q, u64 rcp) {
     return j;
 }
 
-__global__ void __launch_bounds__(kSieveThreads) k_sieve(SieveArgs a, SieveTables t, u64* surv, u32* surv_item,
-                                                         u64 cap, Counters* ctr) {
-    __shared__ u32 bits[kSegWords];
-    __shared__ u32 med_start[kNumMedium];
-    __shared__ u32 warp_sum[kSieveThreads / 32];
-    __shared__ unsigned long long block_base;
-    const u32 tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+struct SieveShared {
+    u32 bits[kSegWords];
+    u32 med_start[kNumMedium];
+    u32 warp_sum[kSieveThreads / 32];
+    unsigned long long block_base;
+};
 
-    if (blockIdx.x == 0 && tid == 0 && a.include_two) {
-        const u64 slot = atomicAdd(&ctr->survivors, 1ull);
-        if (slot < cap) {
-            surv[slot] = 2;
-            if (surv_item) surv_item[slot] = a.item;
-        } else {
-            atomicOr(&ctr->status, kStatusSurvivorOverflow);
-        }
+__device__ __forceinline__ void emit_two(u32 item, u64* surv, u32* surv_item, u64 cap, Counters* ctr) {
+    const u64 slot = atomicAdd(&ctr->survivors, 1ull);
+    if (slot < cap) {
+        surv[slot] = 2;
+        if (surv_item) surv_item[slot] = item;
+    } else {
+        atomicOr(&ctr->status, kStatusSurvivorOverflow);
     }
+}
 
-    const u32 n_med = min(a.n_primes, kNumMedium);
-    for (u64 seg = blockIdx.x; seg * kSegOdds < a.n_odds; seg += gridDim.x) {
-        const u64 base = seg * kSegOdds;
-        const u32 len = (u32)min((u64)kSegOdds, a.n_odds - base);
-        const u64 v0 = a.lo_odd + 2 * base;
-
-        // 1. primes 3..31: each thread writes whole words (pattern << offset).
-        {
-            u32 pat[kNumPattern], off[kNumPattern], step[kNumPattern], qs[kNumPattern];
+// One segment of len <= kSegOdds odd numbers v0, v0 + 2, ... (v0 odd, >= 3),
+// sieved by the first n_primes odd primes; survivors appended to surv[].
+// Called by all threads of the block.
+__device__ void sieve_segment(SieveShared& sh, u64 v0, u32 len, u32 n_primes, u32 item, const SieveTables& t,
+                              u64* surv, u32* surv_item, u64 cap, Counters* ctr) {
+    const u32 tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const u32 n_med = min(n_primes, kNumMedium);
+    // 1. primes 3..31: each thread writes whole words (pattern << offset).
+    {
+        u32 pat[kNumPattern], off[kNumPattern], step[kNumPattern], qs[kNumPattern];
+#pragma unroll
+        for (u32 k = 0; k < kNumPattern; ++k) {
+            const u32 q = t.sp[k];
+            qs[k] = q;
+            u32 pm = 0;
+            for (u32 b = 0; b < 32; b += q) pm |= 1u << b;
+            pat[k] = pm;
+            const u32 j0 = first_odd_multiple(v0, q, t.rcp[k]);
+            int o = (int)j0 - (int)((32u * tid) % q);   // word w = tid first
+            if (o < 0) o += (int)q;
+            off[k] = (u32)o;
+            step[k] = (32u * kSieveThreads) % q;
+        }
+        for (u32 w = tid; w < kSegWords; w += kSieveThreads) {
+            u32 word = 0;
 #pragma unroll
             for (u32 k = 0; k < kNumPattern; ++k) {
-                const u32 q = t.sp[k];
-                qs[k] = q;
-                u32 pm = 0;
-                for (u32 b = 0; b < 32; b += q) pm |= 1u << b;
-                pat[k] = pm;
-                const u32 j0 = first_odd_multiple(v0, q, t.rcp[k]);
-                int o = (int)j0 - (int)((32u * tid) % q);   // word w = tid first
-                if (o < 0) o += (int)q;
+                word |= pat[k] << off[k];
+                int o = (int)off[k] - (int)step[k];
+                if (o < 0) o += (int)qs[k];
                 off[k] = (u32)o;
-                step[k] = (32u * kSieveThreads) % q;
             }
-            for (u32 w = tid; w < kSegWords; w += kSieveThreads) {
-                u32 word = 0;
-#pragma unroll
-                for (u32 k = 0; k < kNumPattern; ++k) {
-                    word |= pat[k] << off[k];
-                    int o = (int)off[k] - (int)step[k];
-                    if (o < 0) o += (int)qs[k];
-                    off[k] = (u32)o;
-                }
-                bits[w] = word;
-            }
+            sh.bits[w] = word;
         }
-        if (tid >= kNumPattern && tid < n_med) med_start[tid] = (u32)min(first_strike(v0, t.sp[tid], t.rcp[tid]), (u64)kSegOdds);
-        __syncthreads();
-        // the pattern struck 3..31 themselves when they lie in this segment
-        if (v0 <= 31 && tid < kNumPattern) {
-            const u32 q = t.sp[tid];
-            if (q >= v0) {
-                const u32 i = (u32)((q - v0) >> 1);
-                if (i < len) atomicAnd(&bits[i >> 5], ~(1u << (i & 31)));
-            }
+    }
+    if (tid >= kNumPattern && tid < n_med)
+        sh.med_start[tid] = (u32)min(first_strike(v0, t.sp[tid], t.rcp[tid]), (u64)kSegOdds);
+    __syncthreads();
+    // the pattern struck 3..31 themselves when they lie in this segment
+    if (v0 <= 31 && tid < kNumPattern) {
+        const u32 q = t.sp[tid];
+        if (q >= v0) {
+            const u32 i = (u32)((q - v0) >> 1);
+            if (i < len) atomicAnd(&sh.bits[i >> 5], ~(1u << (i & 31)));
         }
+    }
+    // 2. primes 37..1021: all threads share each prime.
+    for (u32 k = kNumPattern; k < n_med; ++k) {
+        const u32 q = t.sp[k];
+        for (u32 i = sh.med_start[k] + tid * q; i < len; i += kSieveThreads * q)
+            atomicOr(&sh.bits[i >> 5], 1u << (i & 31));
+    }
+    // 3. primes 1031..65521: one thread per prime.
+    for (u32 k = kNumMedium + tid; k < n_primes; k += kSieveThreads) {
+        const u32 q = t.sp[k];
+        const u64 j = first_strike(v0, q, t.rcp[k]);
+        for (u64 i = j; i < len; i += q) atomicOr(&sh.bits[(u32)i >> 5], 1u << ((u32)i & 31));
+    }
+    __syncthreads();
 
-        // 2. primes 37..1021: all threads share each prime.
-        for (u32 k = kNumPattern; k < n_med; ++k) {
-            const u32 q = t.sp[k];
-            for (u32 i = med_start[k] + tid * q; i < len; i += kSieveThreads * q)
-                atomicOr(&bits[i >> 5], 1u << (i & 31));
+    // 4. survivors: contiguous words per thread, block scan, one global atomic.
+    const u32 w0 = tid * kWordsPerThread;
+    u32 mine = 0;
+#pragma unroll
+    for (u32 k = 0; k < kWordsPerThread; ++k) {
+        const u32 w = w0 + k;
+        u32 x = ~sh.bits[w];
+        const u32 first = w * 32;
+        if (first >= len) x = 0;
+        else if (len - first < 32) x &= (1u << (len - first)) - 1u;
+        mine += __popc(x);
+    }
+    u32 incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const u32 y = __shfl_up_sync(FULL, incl, o);
+        if (lane >= (u32)o) incl += y;
+    }
+    if (lane == 31) sh.warp_sum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        u32 ws = lane < kSieveThreads / 32 ? sh.warp_sum[lane] : 0;
+        u32 wincl = ws;
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) {
+            const u32 y = __shfl_up_sync(FULL, wincl, o);
+            if (lane >= (u32)o) wincl += y;
         }
-        // 3. primes 1031..65521: one thread per prime.
-        for (u32 k = kNumMedium + tid; k < a.n_primes; k += kSieveThreads) {
-            const u32 q = t.sp[k];
-            const u64 j = first_strike(v0, q, t.rcp[k]);
-            for (u64 i = j; i < len; i += q) atomicOr(&bits[(u32)i >> 5], 1u << ((u32)i & 31));
+        if (lane < kSieveThreads / 32) sh.warp_sum[lane] = wincl - ws;   // exclusive
+        if (lane == kSieveThreads / 32 - 1) sh.block_base = atomicAdd(&ctr->survivors, (unsigned long long)wincl);
+    }
+    __syncthreads();
+    u64 pos = sh.block_base + sh.warp_sum[warp] + (incl - mine);
+    for (u32 k = 0; k < kWordsPerThread; ++k) {
+        const u32 w = w0 + k;
+        u32 x = ~sh.bits[w];
+        const u32 first = w * 32;
+        if (first >= len) x = 0;
+        else if (len - first < 32) x &= (1u << (len - first)) - 1u;
+        while (x) {
+            const u32 b = __ffs(x) - 1;
+            x &= x - 1;
+            if (pos < cap) {
+                surv[pos] = v0 + 2ull * (first + b);
+                if (surv_item) surv_item[pos] = item;
+            }
+            ++pos;
         }
-        __syncthreads();
+    }
+    if (pos > cap) atomicOr(&ctr->status, kStatusSurvivorOverflow);
+    __syncthreads();
+}
 
-        // 4. survivors: contiguous words per thread, block scan, one global atomic.
-        const u32 w0 = tid * kWordsPerThread;
-        u32 mine = 0;
-#pragma unroll
-        for (u32 k = 0; k < kWordsPerThread; ++k) {
-            const u32 w = w0 + k;
-            u32 x = ~bits[w];
-            const u32 first = w * 32;
-            if (first >= len) x = 0;
-            else if (len - first < 32) x &= (1u << (len - first)) - 1u;
-            mine += __popc(x);
+__global__ void __launch_bounds__(kSieveThreads) k_sieve(SieveArgs a, SieveTables t, u64* surv, u32* surv_item,
+                                                         u64 cap, Counters* ctr) {
+    __shared__ SieveShared sh;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && a.include_two) emit_two(a.item, surv, surv_item, cap, ctr);
+    for (u64 seg = blockIdx.x; seg * kSegOdds < a.n_odds; seg += gridDim.x) {
+        const u64 base = seg * kSegOdds;
+        sieve_segment(sh, a.lo_odd + 2 * base, (u32)min((u64)kSegOdds, a.n_odds - base), a.n_primes, a.item, t, surv,
+                      surv_item, cap, ctr);
+    }
+}
+
+// The same over a wave of runs (ranges of possibly different items), read
+// from device memory so that a captured graph can be replayed per wave.
+__global__ void __launch_bounds__(kSieveThreads) k_sieve_wave(const WaveDesc* w, SieveTables t, u64* surv,
+                                                              u32* surv_item, u64 cap, Counters* ctr) {
+    __shared__ SieveShared sh;
+    const u32 n_runs = w->n_runs;
+    const u64 total = w->total_segs;
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        for (u32 r = 0; r < n_runs; ++r)
+            if (w->runs[r].include_two) emit_two(w->runs[r].item, surv, surv_item, cap, ctr);
+    for (u64 seg = blockIdx.x; seg < total; seg += gridDim.x) {
+        u32 lo = 0, hi = n_runs;                        // last run with seg_begin <= seg
+        while (hi - lo > 1) {
+            const u32 mid = (lo + hi) >> 1;
+            if (w->runs[mid].seg_begin <= seg) lo = mid;
+            else hi = mid;
         }
-        u32 incl = mine;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const u32 y = __shfl_up_sync(FULL, incl, o);
-            if (lane >= (u32)o) incl += y;
-        }
-        if (lane == 31) warp_sum[warp] = incl;
-        __syncthreads();
-        if (warp == 0) {
-            u32 ws = lane < kSieveThreads / 32 ? warp_sum[lane] : 0;
-            u32 wincl = ws;
-#pragma unroll
-            for (int o = 1; o < 8; o <<= 1) {
-                const u32 y = __shfl_up_sync(FULL, wincl, o);
-                if (lane >= (u32)o) wincl += y;
-            }
-            if (lane < kSieveThreads / 32) warp_sum[lane] = wincl - ws;   // exclusive
-            if (lane == kSieveThreads / 32 - 1) block_base = atomicAdd(&ctr->survivors, (unsigned long long)wincl);
-        }
-        __syncthreads();
-        u64 pos = block_base + warp_sum[warp] + (incl - mine);
-        for (u32 k = 0; k < kWordsPerThread; ++k) {
-            const u32 w = w0 + k;
-            u32 x = ~bits[w];
-            const u32 first = w * 32;
-            if (first >= len) x = 0;
-            else if (len - first < 32) x &= (1u << (len - first)) - 1u;
-            while (x) {
-                const u32 b = __ffs(x) - 1;
-                x &= x - 1;
-                if (pos < cap) {
-                    surv[pos] = v0 + 2ull * (first + b);
-                    if (surv_item) surv_item[pos] = a.item;
-                }
-                ++pos;
-            }
-        }
-        if (pos > cap) atomicOr(&ctr->status, kStatusSurvivorOverflow);
-        __syncthreads();
+        const SieveRun& run = w->runs[lo];
+        const u64 base = (seg - run.seg_begin) * kSegOdds;
+        if (base >= run.n_odds) continue;               // (a run with no odd numbers)
+        sieve_segment(sh, run.lo_odd + 2 * base, (u32)min((u64)kSegOdds, run.n_odds - base), run.n_primes, run.item, t,
+                      surv, surv_item, cap, ctr);
     }
 }
 
@@ -829,6 +864,8 @@ __device__ u64 solve_fp64(const Entry& e, u32* tab, u32 tbits, u64* steps_out) {
     f.init(e.p);
     const u32 m = e.m;
     const u32 jc = (u32)e.jcount;                      // jcount <= 10^7
+    // this prime's table: 2^tb slots for m baby steps (load <= ~1/5), at most the launch's
+    tbits = min(tbits, max(6u, 32u - __clz(5 * m - 1)));
     const u32 mask = (1u << tbits) - 1, shift = 32 - tbits;
     const double B = (double)e.B, Bm = (double)e.Bm, tv = (double)e.t, G0 = (double)e.G0;
 
@@ -1285,16 +1322,35 @@ cudaError_t launch_sieve(const SieveArgs& a, const SieveTables& t, u64* surv, u3
     return cudaGetLastError();
 }
 
+cudaError_t launch_sieve_wave(const WaveDesc* w, const SieveTables& t, u64* surv, u32* surv_item, u64 surv_cap,
+                              Counters* ctr, int grid, cudaStream_t s) {
+    k_sieve_wave<<<grid, kSieveThreads, 0, s>>>(w, t, surv, surv_item, surv_cap, ctr);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_prep(const PrepArgs& a, Counters* ctr, int grid, cudaStream_t s) {
     k_prep<<<grid, kPrepThreads, 0, s>>>(a, ctr);
     return cudaGetLastError();
 }
 
-cudaError_t launch_bsgs(const BsgsArgs& a, Counters* ctr, int grid, cudaStream_t s) {
-    const size_t smem = bsgs_smem_bytes(a.tbits, a.warps_per_block);
-    auto go = [&](auto kern) {
+// Dynamic shared memory limit of every k_bsgs variant (set once per size,
+// before any graph capture; a set during capture is not needed then).
+cudaError_t bsgs_reserve_smem(size_t smem) {
+    static size_t done = 0;
+    if (smem <= done) return cudaSuccess;
+    for (auto kern : {k_bsgs<0>, k_bsgs<1>, k_bsgs<2>, k_bsgs<4>}) {
         cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (err != cudaSuccess) return err;
+    }
+    done = smem;
+    return cudaSuccess;
+}
+
+cudaError_t launch_bsgs(const BsgsArgs& a, Counters* ctr, int grid, cudaStream_t s) {
+    const size_t smem = bsgs_smem_bytes(a.tbits, a.warps_per_block);
+    cudaError_t err = bsgs_reserve_smem(smem);
+    if (err != cudaSuccess) return err;
+    auto go = [&](auto kern) {
         kern<<<grid, a.warps_per_block * 32, smem, s>>>(a, ctr);
         return cudaGetLastError();
     };

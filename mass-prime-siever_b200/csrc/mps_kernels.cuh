@@ -27,6 +27,28 @@ struct SieveArgs {
 cudaError_t launch_sieve(const SieveArgs& a, const SieveTables& t, u64* surv, u32* surv_item, u64 surv_cap,
                          Counters* ctr, cudaStream_t s);
 
+// A wave: several runs (odd ranges of possibly different items) sieved by
+// one launch; kept in device memory so that a captured graph is replayable.
+constexpr u32 kMaxRuns = 512;
+struct SieveRun {
+    u64 lo_odd;        // first odd >= max(lo, 3)
+    u64 n_odds;
+    u64 seg_begin;     // index of this run's first segment in the wave
+    u32 n_primes;
+    u32 include_two;
+    u32 item;
+    u32 pad;
+};
+struct WaveDesc {
+    u32 n_runs;
+    u32 pad;
+    u64 total_segs;
+    SieveRun runs[kMaxRuns];
+};
+constexpr u64 kSieveSegOdds = 65536;   // odd numbers per sieve segment (one block)
+cudaError_t launch_sieve_wave(const WaveDesc* w, const SieveTables& t, u64* surv, u32* surv_item, u64 surv_cap,
+                              Counters* ctr, int grid, cudaStream_t s);
+
 // Prep: filters, primality screen and BSGS set-up for every survivor.
 struct PrepArgs {
     const u64* surv;
@@ -55,6 +77,7 @@ struct BsgsArgs {
     u64 max_p;                 // largest p of the entries (>= 2^49: integer solve)
 };
 cudaError_t launch_bsgs(const BsgsArgs& a, Counters* ctr, int grid, cudaStream_t s);
+cudaError_t bsgs_reserve_smem(size_t smem);   // call before capturing a launch_bsgs
 
 // Order q = ord_p(b) and the exact 12-base primality check of every relation.
 struct OrderArgs {

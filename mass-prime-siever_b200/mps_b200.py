@@ -102,6 +102,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.mps_filter.argtypes = [vp, P(u64), sz, P(Item), P(ctypes.c_uint8)]
     L.mps_batch_relations.argtypes = [vp, P(Item), sz, P(Relation), P(u32), sz, P(sz)]
     L.mps_count_primes.argtypes = [vp, u64, u64, P(u64)]
+    L.mps_take_relations.argtypes = [vp, P(Relation), P(u32), sz, P(sz)]
     L.mps_measure_peaks.argtypes = [vp, P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_double)]
     L.mps_test_survivors.argtypes = [vp, u64, u64, P(u64), sz, P(sz)]
     L.mps_test_is_prime.argtypes = [vp, P(u64), sz, P(ctypes.c_uint8)]
@@ -168,16 +169,22 @@ class Siever:
         self._check(self.lib.mps_get_stats(self.ctx, ctypes.byref(s)))
         return {k: getattr(s, k) for k, _ in Stats._fields_}
 
+    def _take(self, count: int, with_items: bool = False):
+        buf = (Relation * max(count, 1))()
+        its = (ctypes.c_uint32 * max(count, 1))() if with_items else None
+        n = ctypes.c_size_t()
+        self._check(self.lib.mps_take_relations(self.ctx, buf, its, count, ctypes.byref(n)))
+        return buf, its, n.value
+
     def _relations(self, fn, *args, cap: int = 1 << 14):
-        while True:
-            buf = (Relation * max(cap, 1))()
-            n = ctypes.c_size_t()
-            rc = fn(self.ctx, *args, buf, cap, ctypes.byref(n))
-            if rc == MPS_E_CAPACITY:
-                cap = n.value
-                continue
+        buf = (Relation * max(cap, 1))()
+        n = ctypes.c_size_t()
+        rc = fn(self.ctx, *args, buf, cap, ctypes.byref(n))
+        if rc == MPS_E_CAPACITY:                      # fetch the kept result, no recomputation
+            buf, _, _ = self._take(n.value)
+        else:
             self._check(rc)
-            return [(buf[i].p, buf[i].M, buf[i].q) for i in range(n.value)]
+        return [(buf[i].p, buf[i].M, buf[i].q) for i in range(n.value)]
 
     def chunk_relations(self, lo: int, hi: int, item: Item):
         return self._relations(self.lib.mps_chunk_relations, lo, hi, ctypes.byref(item))
@@ -205,16 +212,15 @@ class Siever:
 
     def batch_relations(self, items: list[Item], cap: int = 1 << 14):
         arr = (Item * max(len(items), 1))(*items)
-        while True:
-            buf = (Relation * max(cap, 1))()
-            its = (ctypes.c_uint32 * max(cap, 1))()
-            n = ctypes.c_size_t()
-            rc = self.lib.mps_batch_relations(self.ctx, arr, len(items), buf, its, cap, ctypes.byref(n))
-            if rc == MPS_E_CAPACITY:
-                cap = n.value
-                continue
+        buf = (Relation * max(cap, 1))()
+        its = (ctypes.c_uint32 * max(cap, 1))()
+        n = ctypes.c_size_t()
+        rc = self.lib.mps_batch_relations(self.ctx, arr, len(items), buf, its, cap, ctypes.byref(n))
+        if rc == MPS_E_CAPACITY:
+            buf, its, _ = self._take(n.value, with_items=True)
+        else:
             self._check(rc)
-            return [(its[i], buf[i].p, buf[i].M, buf[i].q) for i in range(n.value)]
+        return [(its[i], buf[i].p, buf[i].M, buf[i].q) for i in range(n.value)]
 
     def count_primes(self, lo: int, hi: int) -> int:
         c = ctypes.c_uint64()
