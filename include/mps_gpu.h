@@ -128,6 +128,42 @@ int mps_batch_relations(mps_ctx* ctx, const mps_item* items, size_t n_items, mps
  * size here.  out_item may be NULL. */
 int mps_take_relations(mps_ctx* ctx, mps_relation* out, uint32_t* out_item, size_t cap, size_t* n_out);
 
+/* ---- serving: continuous batching of Factor= items (no counterpart in the reference) ----
+ * A server owns a device context and a worker thread.  Submitted items wait
+ * until admitted (fewer than max_active in flight and their pieces' device
+ * memory within mem_budget_bytes); every wave takes one piece of
+ * piece_odds odd numbers from each in-flight item in turn, so items that
+ * arrive while others run join the next wave.  Per-item progress is kept
+ * in a device table (mps_serve_checkpoint).  Results equal
+ * mps_item_relations on the same item. */
+typedef struct mps_server mps_server;
+typedef struct mps_serve_config {
+    uint32_t struct_size;       /* sizeof(mps_serve_config)                  */
+    uint32_t max_active;        /* items in flight at once (0: 256)           */
+    uint64_t mem_budget_bytes;  /* device memory for in-flight items (0: 4 GiB) */
+    uint64_t piece_odds;        /* odd numbers per item piece (0: 2^22)       */
+    uint32_t reserved[8];
+} mps_serve_config;
+typedef struct mps_serve_status {
+    uint64_t ticket;
+    int32_t  state;             /* 0 queued, 1 running, 2 done, 3 failed      */
+    int32_t  error;
+    uint64_t p_done;
+    uint64_t relations;
+    double   latency_ms;        /* submit -> done                             */
+    double   queue_ms;          /* submit -> admitted                         */
+} mps_serve_status;
+int mps_serve_config_default(mps_serve_config* cfg);
+int mps_serve_open(int device, const mps_tuning* tuning, const mps_serve_config* cfg, mps_server** out);
+int mps_serve_submit(mps_server* sv, const mps_item* item, uint64_t* ticket);
+/* MPS_OK when done, MPS_E_TIMEOUT if still running after timeout_s. */
+int mps_serve_wait(mps_server* sv, uint64_t ticket, double timeout_s, mps_serve_status* status);
+int mps_serve_result(mps_server* sv, uint64_t ticket, mps_relation* out, size_t cap, size_t* n_out);
+int mps_serve_release(mps_server* sv, uint64_t ticket);
+/* Device-resident progress of an item: every p below *p_done sieved, *n_rel relations. */
+int mps_serve_checkpoint(mps_server* sv, uint64_t ticket, uint64_t* p_done, uint64_t* n_rel);
+int mps_serve_close(mps_server* sv);
+
 /* Number of primes in [lo, hi) counted on the device (the unit of the
  * sieved-primes/s metric; not part of the relation path). */
 int mps_count_primes(mps_ctx* ctx, uint64_t lo, uint64_t hi, uint64_t* count);

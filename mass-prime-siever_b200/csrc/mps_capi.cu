@@ -9,10 +9,17 @@
 #include "mps_kernels.cuh"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <set>
 #include <string>
+#include <thread>
 #include <vector>
 
 using namespace mps;
@@ -77,6 +84,7 @@ struct WaveSlot {
     cudaGraphExec_t graph = nullptr;
     u32 graph_tbits = 0;
     const DevItem* graph_items = nullptr;
+    const ItemState* graph_state = nullptr;
     bool busy = false;
     std::vector<std::pair<u64, u64>> ranges;   // (lo, hi) of each run in flight
     std::vector<u32> range_item;
@@ -108,6 +116,7 @@ struct mps_ctx {
     u64 rel_cap = 0;
     DevItem* d_items = nullptr;
     u64 items_cap = 0;
+    ItemState* d_state = nullptr;      // per-item progress, same capacity as d_items
     WaveSlot slot[2];
     bool slots_ready = false;
     std::vector<u64> item_K;           // K of each item on the device (table sizing)
@@ -242,9 +251,23 @@ u32 sieve_prime_count(u64 hi) {
     return n;
 }
 
+int reserve_items(mps_ctx* c, size_t n) {
+    if (c->items_cap >= n && c->d_items) return MPS_OK;
+    for (WaveSlot& w : c->slot)
+        if (w.stream) CK(cudaStreamSynchronize(w.stream), "wave");
+    if (c->d_state) CK(cudaFree(c->d_state), "cudaFree");
+    c->d_state = nullptr;
+    const u64 cap = std::max<u64>(n, 64);
+    if (int r = ensure(c, &c->d_items, &c->items_cap, cap, "item buffer")) return r;
+    CK(cudaMalloc((void**)&c->d_state, cap * sizeof(ItemState)), "item state");
+    return MPS_OK;
+}
+
 int upload_items(mps_ctx* c, const DevItem* items, size_t n) {
-    if (int r = ensure(c, &c->d_items, &c->items_cap, std::max<u64>(n, 1), "item buffer")) return r;
+    if (int r = reserve_items(c, std::max<size_t>(n, 1))) return r;
     CK(cudaMemcpyAsync(c->d_items, items, n * sizeof(DevItem), cudaMemcpyHostToDevice, c->stream), "item upload");
+    CK(cudaMemsetAsync(c->d_state, 0, n * sizeof(ItemState), c->stream), "item state reset");
+    CK(cudaStreamSynchronize(c->stream), "item upload");
     return MPS_OK;
 }
 
@@ -467,6 +490,7 @@ int slot_enqueue(mps_ctx* c, WaveSlot& w, u32 tbits, bool capturing) {
     CK(launch_bsgs(ba, w.d_ctr, bgrid, s), "bsgs launch");
     CK(cudaEventRecordWithFlags(w.ev_b1, s, ev_flags), "event");
     CK(launch_order(oa, w.d_ctr, grid_for(c, 4), s), "order launch");
+    CK(launch_commit(w.d_wave, w.d_rel, w.d_ctr, w.rel_cap, c->d_state, s), "commit launch");
     CK(cudaMemcpyAsync(w.h_ctr, w.d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, s), "count read");
     CK(cudaMemcpyAsync(w.h_rel, w.d_rel, kGraphRelations * sizeof(RawRelation), cudaMemcpyDeviceToHost, s),
        "relation read");
@@ -475,7 +499,7 @@ int slot_enqueue(mps_ctx* c, WaveSlot& w, u32 tbits, bool capturing) {
 
 int slot_launch(mps_ctx* c, WaveSlot& w, u32 tbits) {
     if (c->tun.reserved[1]) return slot_enqueue(c, w, tbits, false);       // graphs off (tuning)
-    if (!w.graph || w.graph_tbits != tbits || w.graph_items != c->d_items) {
+    if (!w.graph || w.graph_tbits != tbits || w.graph_items != c->d_items || w.graph_state != c->d_state) {
         if (w.graph) cudaGraphExecDestroy(w.graph);
         w.graph = nullptr;
         CK(bsgs_reserve_smem(bsgs_smem_bytes(tbits, c->tun.bsgs_warps)), "bsgs shared memory");
@@ -493,6 +517,7 @@ int slot_launch(mps_ctx* c, WaveSlot& w, u32 tbits) {
         if (e != cudaSuccess) return cuda_fail(c, e, "graph instantiate");
         w.graph_tbits = tbits;
         w.graph_items = c->d_items;
+        w.graph_state = c->d_state;
     }
     CK(cudaGraphLaunch(w.graph, w.stream), "graph launch");
     return MPS_OK;
@@ -509,7 +534,7 @@ int slot_finish(mps_ctx* c, WaveSlot& w, std::vector<RawRelation>& out) {
     CK(cudaEventElapsedTime(&bms, w.ev_b0, w.ev_b1), "event time");
     c->stats.bsgs_ms += bms;
     c->stats.bsgs_launches += 1;
-    c->stats.kernel_launches += 4;
+    c->stats.kernel_launches += 5;
     if (h.status & kStatusOrderFailed) return fail(c, MPS_E_CUDA, "order computation did not factor p - 1");
     if (h.status & (kStatusSurvivorOverflow | kStatusEntryOverflow | kStatusRelationOverflow)) {
         for (size_t i = 0; i < w.ranges.size(); ++i) {
@@ -591,6 +616,7 @@ int run_waves(mps_ctx* c, const std::vector<u64>& lo, const std::vector<u64>& hi
             run.n_primes = sieve_prime_count(b);
             run.item = (u32)i;
             run.pad = 0;
+            run.hi = b;
             cur->ranges.push_back({a, b});
             cur->range_item.push_back((u32)i);
             wave_odds += run.n_odds;
@@ -605,6 +631,238 @@ int run_waves(mps_ctx* c, const std::vector<u64>& lo, const std::vector<u64>& hi
         if (int r = slot_finish(c, c->slot[(k + j) & 1], out)) return r;
     return MPS_OK;
 }
+
+
+// ---------------------------------------------------------------- serving --
+//
+// A server owns a context and a worker thread.  Submitted items wait in a
+// queue until admitted: an item is admitted while fewer than max_active items
+// are in flight and the device memory its pieces need -- survivors and BSGS
+// entries of one piece of its P range, plus its baby-step tables for the
+// resident warps -- fits the budget left by the items already in flight.
+// Every wave takes one piece from each in-flight item in turn (continuous
+// batching: items admitted while others run join the next wave), so short
+// items finish after a few waves while long ones keep going.  Each item's
+// progress (P sieved, relations found) lives in a device table updated by
+// the commit kernel at the end of every wave; relations are mirrored to the
+// host as waves complete.
+
+}  // namespace
+
+struct ServeReq {
+    u64 ticket = 0;
+    mps_item item{};
+    DevItem d{};
+    int slot = -1;                     // device item index while in flight
+    u64 cursor = 0;                    // next P to hand to a wave
+    u32 inflight = 0;                  // waves in flight with a piece of this item
+    std::multiset<u64> piece_lo;       // low ends of this item's pieces in flight
+    u64 mem = 0;                       // device bytes reserved
+    int state = 0;                     // 0 queued, 1 active, 2 done, 3 failed
+    int error = 0;
+    std::vector<RawRelation> rel;
+    std::chrono::steady_clock::time_point t_submit, t_admit, t_done;
+};
+
+struct mps_server {
+    mps_ctx* ctx = nullptr;
+    mps_serve_config cfg{};
+    std::thread worker;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<u64> queue;
+    std::map<u64, ServeReq> reqs;
+    std::vector<u64> slot_owner;       // device item slot -> ticket (0: free)
+    u64 next_ticket = 1;
+    u64 mem_used = 0;
+    u32 active = 0;
+    bool stop = false;
+    int fatal = 0;
+    std::string fatal_msg;
+    std::vector<u64> wave_tickets[2];  // tickets with a piece in each slot's wave
+};
+
+namespace {
+
+double ms_between(std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+    return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+// Device bytes an item's pieces need: survivors (8 B) and entries (72 B) of
+// one piece (density of survivors ~ 2.2/ln(P0) of the odd numbers, at most
+// all of them below 10^6), and 4-byte table slots for the resident warps.
+u64 item_memory(const mps_server* sv, const DevItem& d, const mps_item& it) {
+    const double lp = std::log((double)std::max<u64>(it.P0, 16));
+    const double dens = std::min(1.0, 2.2 / lp + (it.P0 < 1000000 ? 0.3 : 0.0));
+    const u64 piece = std::min<u64>(sv->cfg.piece_odds, (it.P1 - it.P0) / 2 + 1);
+    u32 tb, mb;
+    table_for(sv->ctx, d.K, &tb, &mb);
+    const u64 tables = (u64)(4u << tb) * 64 * (u64)sv->ctx->num_sms;   // resident warps x slots x 4 B
+    return (u64)(piece * dens * (8.0 + 72.0 * 0.5)) + tables / 16 + sizeof(DevItem) + sizeof(ItemState);
+}
+
+void serve_route(mps_server* sv, int k, std::vector<RawRelation>& rel, const WaveSlot& w) {
+    for (size_t i = 0; i < w.ranges.size(); ++i) {
+        auto it = sv->reqs.find(sv->slot_owner[w.range_item[i]]);
+        if (it == sv->reqs.end()) continue;
+        auto pos = it->second.piece_lo.find(w.ranges[i].first);
+        if (pos != it->second.piece_lo.end()) it->second.piece_lo.erase(pos);
+    }
+    for (const RawRelation& r : rel) {
+        const u64 t = sv->slot_owner[r.item];
+        auto it = sv->reqs.find(t);
+        if (it != sv->reqs.end()) it->second.rel.push_back(r);
+    }
+    for (u64 t : sv->wave_tickets[k]) {
+        auto it = sv->reqs.find(t);
+        if (it == sv->reqs.end()) continue;
+        ServeReq& q = it->second;
+        if (q.inflight) --q.inflight;
+        if (q.state == 1 && q.inflight == 0 && q.cursor >= q.item.P1) {
+            q.state = 2;
+            q.t_done = std::chrono::steady_clock::now();
+            std::sort(q.rel.begin(), q.rel.end(), [](const RawRelation& a, const RawRelation& b) { return a.p < b.p; });
+            sv->slot_owner[q.slot] = 0;
+            sv->mem_used -= q.mem;
+            --sv->active;
+        }
+    }
+    sv->wave_tickets[k].clear();
+}
+
+void serve_fail_all(mps_server* sv, int code, const std::string& msg) {
+    sv->fatal = code;
+    sv->fatal_msg = msg;
+    for (auto& kv : sv->reqs)
+        if (kv.second.state < 2) {
+            kv.second.state = 3;
+            kv.second.error = code;
+            kv.second.t_done = std::chrono::steady_clock::now();
+        }
+    sv->queue.clear();
+}
+
+void serve_loop(mps_server* sv) {
+    mps_ctx* c = sv->ctx;
+    cudaSetDevice(c->device);
+    const u64 chunk = c->tun.chunk_odds;
+    u32 tbits = 11;
+    {
+        u32 mb;
+        table_for(c, 10000000ull, &tbits, &mb);       // the widest N range sets the launch's table size
+    }
+    int k = 0;
+    std::unique_lock<std::mutex> lk(sv->mu);
+    for (;;) {
+        // admission
+        while (!sv->queue.empty() && sv->active < sv->cfg.max_active) {
+            ServeReq& q = sv->reqs[sv->queue.front()];
+            if (sv->active > 0 && sv->mem_used + q.mem > sv->cfg.mem_budget_bytes) break;
+            int slot = -1;
+            for (size_t i = 0; i < sv->slot_owner.size(); ++i)
+                if (sv->slot_owner[i] == 0) {
+                    slot = (int)i;
+                    break;
+                }
+            if (slot < 0) break;
+            sv->queue.pop_front();
+            q.slot = slot;
+            q.d.item_index = (u32)slot;
+            sv->slot_owner[slot] = q.ticket;
+            sv->mem_used += q.mem;
+            ++sv->active;
+            q.state = 1;
+            q.cursor = q.item.P0;
+            q.t_admit = std::chrono::steady_clock::now();
+            c->item_K[slot] = q.d.K;
+            cudaError_t e = cudaMemcpy(c->d_items + slot, &q.d, sizeof(DevItem), cudaMemcpyHostToDevice);
+            if (e == cudaSuccess) e = cudaMemset(c->d_state + slot, 0, sizeof(ItemState));
+            if (e != cudaSuccess) {
+                serve_fail_all(sv, MPS_E_CUDA, std::string("item upload: ") + cudaGetErrorString(e));
+                break;
+            }
+        }
+        // pieces of every in-flight item with P left, round robin
+        std::vector<ServeReq*> work;
+        for (auto& kv : sv->reqs)
+            if (kv.second.state == 1 && kv.second.cursor < kv.second.item.P1) work.push_back(&kv.second);
+        const bool any_inflight = c->slot[0].busy || c->slot[1].busy;
+        if (work.empty() && !any_inflight) {
+            if (sv->stop && sv->queue.empty()) break;
+            sv->cv_done.notify_all();
+            sv->cv_work.wait_for(lk, std::chrono::milliseconds(20));
+            continue;
+        }
+        WaveSlot& w = c->slot[k];
+        // the slot's previous wave: wait without the lock, then route
+        if (w.busy) {
+            std::vector<RawRelation> rel;
+            lk.unlock();
+            const int r = slot_finish(c, w, rel);
+            lk.lock();
+            if (r) {
+                serve_fail_all(sv, r, c->err);
+                sv->cv_done.notify_all();
+                break;
+            }
+            serve_route(sv, k, rel, w);
+            sv->cv_done.notify_all();
+        }
+        if (!work.empty()) {
+            w.h_wave->n_runs = 0;
+            w.ranges.clear();
+            w.range_item.clear();
+            u64 wave_odds = 0;
+            const u64 quantum = std::max<u64>(sv->cfg.piece_odds, chunk / std::max<size_t>(work.size(), 1));
+            for (bool more = true; more && wave_odds < chunk && w.h_wave->n_runs < kMaxRuns;) {
+                more = false;
+                for (ServeReq* q : work) {
+                    if (q->cursor >= q->item.P1 || wave_odds >= chunk || w.h_wave->n_runs >= kMaxRuns) continue;
+                    const u64 a = q->cursor;
+                    const u64 lo_odd = std::max<u64>(a, 3) | 1ull;
+                    const u64 take = std::min<u64>(quantum, chunk - wave_odds);
+                    u64 b = q->item.P1;
+                    if (lo_odd < b && (b - lo_odd + 1) / 2 > take) b = lo_odd + 2 * take;
+                    SieveRun& run = w.h_wave->runs[w.h_wave->n_runs++];
+                    run.lo_odd = lo_odd;
+                    run.n_odds = lo_odd < b ? (b - lo_odd + 1) / 2 : 0;
+                    run.include_two = (a <= 2 && b > 2) ? 1 : 0;
+                    run.n_primes = sieve_prime_count(b);
+                    run.item = (u32)q->slot;
+                    run.pad = 0;
+                    run.hi = b;
+                    w.ranges.push_back({a, b});
+                    w.range_item.push_back((u32)q->slot);
+                    wave_odds += run.n_odds;
+                    c->stats.odds += run.n_odds;
+                    q->cursor = b;
+                    q->piece_lo.insert(a);
+                    if (std::find(sv->wave_tickets[k].begin(), sv->wave_tickets[k].end(), q->ticket) ==
+                        sv->wave_tickets[k].end()) {
+                        sv->wave_tickets[k].push_back(q->ticket);
+                        ++q->inflight;
+                    }
+                    if (q->cursor < q->item.P1) more = true;
+                }
+            }
+            w.h_wave->total_segs = 0;
+            for (u32 r = 0; r < w.h_wave->n_runs; ++r) {
+                w.h_wave->runs[r].seg_begin = w.h_wave->total_segs;
+                w.h_wave->total_segs += (w.h_wave->runs[r].n_odds + kSieveSegOdds - 1) / kSieveSegOdds;
+            }
+            const int r = slot_launch(c, w, tbits);
+            if (r) {
+                serve_fail_all(sv, r, c->err);
+                sv->cv_done.notify_all();
+                break;
+            }
+            w.busy = true;
+        }
+        k ^= 1;
+    }
+    sv->cv_done.notify_all();
+}
+
 
 int check_ctx(mps_ctx* c) {
     if (!c) return MPS_E_ARG;
@@ -741,7 +999,7 @@ int mps_close(mps_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (WaveSlot& w : c->slot) slot_free(w);
     for (void* p : {(void*)c->d_sp, (void*)c->d_rcp, (void*)c->d_inv, (void*)c->d_ctr, (void*)c->d_surv,
-                    (void*)c->d_surv_item, (void*)c->d_ent, (void*)c->d_rel, (void*)c->d_items})
+                    (void*)c->d_surv_item, (void*)c->d_ent, (void*)c->d_rel, (void*)c->d_items, (void*)c->d_state})
         if (p) cudaFree(p);
     if (c->h_ctr) cudaFreeHost(c->h_ctr);
     if (c->h_rel) cudaFreeHost(c->h_rel);
@@ -900,6 +1158,169 @@ int mps_take_relations(mps_ctx* c, mps_relation* out, uint32_t* out_item, size_t
     if (!c) return MPS_E_ARG;
     if (!out && cap) return fail(c, MPS_E_ARG, "out is NULL");
     return copy_out(c, c->last, out, out_item, cap, n_out);
+}
+
+
+int mps_serve_config_default(mps_serve_config* cfg) {
+    if (!cfg) return MPS_E_ARG;
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->struct_size = sizeof(mps_serve_config);
+    cfg->max_active = 256;
+    cfg->mem_budget_bytes = 4ull << 30;
+    cfg->piece_odds = 1ull << 22;
+    return MPS_OK;
+}
+
+int mps_serve_open(int device, const mps_tuning* tuning, const mps_serve_config* cfg, mps_server** out) {
+    if (!out) return MPS_E_ARG;
+    *out = nullptr;
+    mps_serve_config conf;
+    mps_serve_config_default(&conf);
+    if (cfg) {
+        if (cfg->struct_size != sizeof(mps_serve_config)) return MPS_E_ARG;
+        if (cfg->max_active) conf.max_active = cfg->max_active;
+        if (cfg->mem_budget_bytes) conf.mem_budget_bytes = cfg->mem_budget_bytes;
+        if (cfg->piece_odds) conf.piece_odds = cfg->piece_odds;
+    }
+    conf.max_active = std::min<u32>(conf.max_active, kMaxRuns);
+    mps_ctx* c = nullptr;
+    if (int r = mps_open(device, tuning, &c)) return r;
+    if (int r = reserve_items(c, conf.max_active)) {
+        mps_close(c);
+        return r;
+    }
+    c->item_K.assign(conf.max_active, 0);
+    for (WaveSlot& w : c->slot)
+        if (int r = slot_alloc(c, w)) {
+            mps_close(c);
+            return r;
+        }
+    c->slots_ready = true;
+    mps_server* sv = new mps_server();
+    sv->ctx = c;
+    sv->cfg = conf;
+    sv->slot_owner.assign(conf.max_active, 0);
+    sv->worker = std::thread(serve_loop, sv);
+    *out = sv;
+    return MPS_OK;
+}
+
+int mps_serve_submit(mps_server* sv, const mps_item* item, uint64_t* ticket) {
+    if (!sv || !item || !ticket) return MPS_E_ARG;
+    ServeReq q;
+    if (int r = make_dev_item(sv->ctx, item, 0, &q.d)) return r;
+    std::lock_guard<std::mutex> g(sv->mu);
+    if (sv->fatal) return MPS_E_STATE;
+    if (sv->stop) return MPS_E_STATE;
+    q.ticket = sv->next_ticket++;
+    q.item = *item;
+    q.mem = item_memory(sv, q.d, *item);
+    q.t_submit = std::chrono::steady_clock::now();
+    *ticket = q.ticket;
+    sv->reqs[q.ticket] = std::move(q);
+    sv->queue.push_back(*ticket);
+    sv->cv_work.notify_one();
+    return MPS_OK;
+}
+
+int mps_serve_wait(mps_server* sv, uint64_t ticket, double timeout_s, mps_serve_status* st) {
+    if (!sv) return MPS_E_ARG;
+    std::unique_lock<std::mutex> lk(sv->mu);
+    auto it = sv->reqs.find(ticket);
+    if (it == sv->reqs.end()) return MPS_E_ARG;
+    const auto deadline = std::chrono::steady_clock::now() + std::chrono::duration<double>(std::max(0.0, timeout_s));
+    while (it->second.state < 2) {
+        if (sv->cv_done.wait_until(lk, deadline) == std::cv_status::timeout && it->second.state < 2) break;
+    }
+    const ServeReq& q = it->second;
+    if (st) {
+        std::memset(st, 0, sizeof(*st));
+        st->ticket = q.ticket;
+        st->state = q.state;
+        st->error = q.error;
+        st->relations = q.rel.size();
+        st->p_done = q.cursor;
+        if (q.state >= 2) {
+            st->latency_ms = ms_between(q.t_submit, q.t_done);
+            st->queue_ms = q.slot >= 0 || q.state == 2 ? ms_between(q.t_submit, q.t_admit) : 0.0;
+        }
+    }
+    if (q.state == 3) return q.error ? q.error : MPS_E_CUDA;
+    return q.state == 2 ? MPS_OK : MPS_E_TIMEOUT;
+}
+
+int mps_serve_result(mps_server* sv, uint64_t ticket, mps_relation* out, size_t cap, size_t* n_out) {
+    if (!sv) return MPS_E_ARG;
+    std::lock_guard<std::mutex> g(sv->mu);
+    auto it = sv->reqs.find(ticket);
+    if (it == sv->reqs.end()) return MPS_E_ARG;
+    const ServeReq& q = it->second;
+    if (q.state != 2) return q.state == 3 ? MPS_E_STATE : MPS_E_TIMEOUT;
+    if (n_out) *n_out = q.rel.size();
+    if (q.rel.size() > cap) return MPS_E_CAPACITY;
+    for (size_t i = 0; i < q.rel.size(); ++i) {
+        out[i].p = q.rel[i].p;
+        out[i].M = q.rel[i].M;
+        out[i].q = q.rel[i].q;
+    }
+    return MPS_OK;
+}
+
+int mps_serve_release(mps_server* sv, uint64_t ticket) {
+    if (!sv) return MPS_E_ARG;
+    std::lock_guard<std::mutex> g(sv->mu);
+    auto it = sv->reqs.find(ticket);
+    if (it == sv->reqs.end()) return MPS_E_ARG;
+    if (it->second.state < 2) return MPS_E_STATE;
+    sv->reqs.erase(it);
+    return MPS_OK;
+}
+
+int mps_serve_checkpoint(mps_server* sv, uint64_t ticket, uint64_t* p_done, uint64_t* n_rel) {
+    if (!sv) return MPS_E_ARG;
+    // The device table holds, per item, the highest P of any committed wave
+    // and the relations committed; pieces are issued in increasing P, so
+    // every P below min(that, the lowest piece still in flight, the next
+    // piece to issue) is sieved.
+    int slot = -1;
+    u64 cursor = 0, nr = 0, limit = 0, P0 = 0;
+    int state = 0;
+    {
+        std::lock_guard<std::mutex> g(sv->mu);
+        auto it = sv->reqs.find(ticket);
+        if (it == sv->reqs.end()) return MPS_E_ARG;
+        const ServeReq& q = it->second;
+        slot = q.slot;
+        state = q.state;
+        cursor = q.state == 2 ? q.item.P1 : q.item.P0;
+        nr = q.rel.size();
+        limit = q.piece_lo.empty() ? q.cursor : *q.piece_lo.begin();
+        P0 = q.item.P0;
+    }
+    if (state == 1 && slot >= 0) {
+        ItemState h{};
+        cudaSetDevice(sv->ctx->device);
+        if (cudaMemcpy(&h, sv->ctx->d_state + slot, sizeof(ItemState), cudaMemcpyDeviceToHost) != cudaSuccess)
+            return MPS_E_CUDA;
+        cursor = std::max<u64>(P0, std::min<u64>(h.p_done, limit));
+        nr = h.n_rel;
+    }
+    if (p_done) *p_done = cursor;
+    if (n_rel) *n_rel = nr;
+    return MPS_OK;
+}
+
+int mps_serve_close(mps_server* sv) {
+    if (!sv) return MPS_E_ARG;
+    {
+        std::lock_guard<std::mutex> g(sv->mu);
+        sv->stop = true;
+        sv->cv_work.notify_all();
+    }
+    if (sv->worker.joinable()) sv->worker.join();
+    mps_close(sv->ctx);
+    delete sv;
+    return MPS_OK;
 }
 
 int mps_count_primes(mps_ctx* c, uint64_t lo, uint64_t hi, uint64_t* count) {

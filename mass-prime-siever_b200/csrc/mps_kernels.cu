@@ -1183,6 +1183,21 @@ __global__ void __launch_bounds__(128) k_order(OrderArgs a, Counters* ctr) {
     }
 }
 
+// ------------------------------------------------------- served-item state --
+
+__global__ void k_commit(const WaveDesc* w, const RawRelation* rel, const Counters* ctr, u64 rel_cap, ItemState* st) {
+    const u32 tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const u32 n_runs = w->n_runs;
+    if (tid < n_runs) {
+        const SieveRun& r = w->runs[tid];
+        atomicMax(&st[r.item].p_done, (unsigned long long)r.hi);
+        atomicAdd(&st[r.item].waves, 1ull);
+    }
+    const u64 n = min((u64)ctr->relations, rel_cap);
+    for (u64 i = tid; i < n; i += (u64)gridDim.x * blockDim.x)
+        if (rel[i].q != ~0ull) atomicAdd(&st[rel[i].item].n_rel, 1ull);
+}
+
 // ------------------------------------------------------ prime counting --
 
 __global__ void __launch_bounds__(256) k_count_primes(const u64* surv, u64 surv_cap, Counters* ctr) {
@@ -1362,6 +1377,12 @@ cudaError_t launch_bsgs(const BsgsArgs& a, Counters* ctr, int grid, cudaStream_t
 
 cudaError_t launch_order(const OrderArgs& a, Counters* ctr, int grid, cudaStream_t s) {
     k_order<<<grid, 128, 0, s>>>(a, ctr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_commit(const WaveDesc* w, const RawRelation* rel, const Counters* ctr, u64 rel_cap,
+                          ItemState* st, cudaStream_t s) {
+    k_commit<<<4, 128, 0, s>>>(w, rel, ctr, rel_cap, st);
     return cudaGetLastError();
 }
 

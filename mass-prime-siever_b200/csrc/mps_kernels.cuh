@@ -34,10 +34,20 @@ struct SieveRun {
     u64 lo_odd;        // first odd >= max(lo, 3)
     u64 n_odds;
     u64 seg_begin;     // index of this run's first segment in the wave
+    u64 hi;            // end of the run's integer range (lo .. hi)
     u32 n_primes;
     u32 include_two;
     u32 item;
     u32 pad;
+};
+
+// Device-resident progress of one served item: every P below p_done is
+// sieved once the wave that covered it has committed; n_rel relations found.
+struct ItemState {
+    unsigned long long p_done;
+    unsigned long long n_rel;
+    unsigned long long waves;
+    unsigned long long pad;
 };
 struct WaveDesc {
     u32 n_runs;
@@ -46,6 +56,9 @@ struct WaveDesc {
     SieveRun runs[kMaxRuns];
 };
 constexpr u64 kSieveSegOdds = 65536;   // odd numbers per sieve segment (one block)
+// After a wave: advance each run's item to the run's end, count relations.
+cudaError_t launch_commit(const WaveDesc* w, const RawRelation* rel, const Counters* ctr, u64 rel_cap,
+                          ItemState* st, cudaStream_t s);
 cudaError_t launch_sieve_wave(const WaveDesc* w, const SieveTables& t, u64* surv, u32* surv_item, u64 surv_cap,
                               Counters* ctr, int grid, cudaStream_t s);
 

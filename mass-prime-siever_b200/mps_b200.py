@@ -61,6 +61,18 @@ class Stats(ctypes.Structure):
     ]
 
 
+class ServeConfig(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_uint32), ("max_active", ctypes.c_uint32),
+                ("mem_budget_bytes", ctypes.c_uint64), ("piece_odds", ctypes.c_uint64),
+                ("reserved", ctypes.c_uint32 * 8)]
+
+
+class ServeStatus(ctypes.Structure):
+    _fields_ = [("ticket", ctypes.c_uint64), ("state", ctypes.c_int32), ("error", ctypes.c_int32),
+                ("p_done", ctypes.c_uint64), ("relations", ctypes.c_uint64),
+                ("latency_ms", ctypes.c_double), ("queue_ms", ctypes.c_double)]
+
+
 def split128(v: int) -> tuple[int, int]:
     if not -(1 << 127) <= v < (1 << 127):
         raise ValueError("value does not fit in a signed 128-bit integer")
@@ -103,6 +115,14 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.mps_batch_relations.argtypes = [vp, P(Item), sz, P(Relation), P(u32), sz, P(sz)]
     L.mps_count_primes.argtypes = [vp, u64, u64, P(u64)]
     L.mps_take_relations.argtypes = [vp, P(Relation), P(u32), sz, P(sz)]
+    L.mps_serve_config_default.argtypes = [P(ServeConfig)]
+    L.mps_serve_open.argtypes = [ctypes.c_int, P(Tuning), P(ServeConfig), P(vp)]
+    L.mps_serve_submit.argtypes = [vp, P(Item), P(u64)]
+    L.mps_serve_wait.argtypes = [vp, u64, ctypes.c_double, P(ServeStatus)]
+    L.mps_serve_result.argtypes = [vp, u64, P(Relation), sz, P(sz)]
+    L.mps_serve_release.argtypes = [vp, u64]
+    L.mps_serve_checkpoint.argtypes = [vp, u64, P(u64), P(u64)]
+    L.mps_serve_close.argtypes = [vp]
     L.mps_measure_peaks.argtypes = [vp, P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_double)]
     L.mps_test_survivors.argtypes = [vp, u64, u64, P(u64), sz, P(sz)]
     L.mps_test_is_prime.argtypes = [vp, P(u64), sz, P(ctypes.c_uint8)]
@@ -263,3 +283,66 @@ class Siever:
         out = (ctypes.c_uint64 * max(len(pairs), 1))()
         self._check(self.lib.mps_test_order(self.ctx, arr, len(pairs), out))
         return list(out[:len(pairs)])
+
+
+class Server:
+    """Continuous-batching server (mps_serve_*): submit items, wait for them."""
+
+    def __init__(self, device: int = 0, tuning: Tuning | None = None, **cfg):
+        self.lib = load_library()
+        conf = ServeConfig()
+        self.lib.mps_serve_config_default(ctypes.byref(conf))
+        for k, v in cfg.items():
+            setattr(conf, k, v)
+        if tuning is None:
+            tuning = default_tuning()
+        self.sv = ctypes.c_void_p()
+        rc = self.lib.mps_serve_open(device, ctypes.byref(tuning), ctypes.byref(conf), ctypes.byref(self.sv))
+        if rc != MPS_OK:
+            raise MpsError(rc, "mps_serve_open failed")
+
+    def submit(self, item: Item) -> int:
+        t = ctypes.c_uint64()
+        rc = self.lib.mps_serve_submit(self.sv, ctypes.byref(item), ctypes.byref(t))
+        if rc != MPS_OK:
+            raise MpsError(rc, "submit")
+        return t.value
+
+    def wait(self, ticket: int, timeout: float = 600.0) -> dict:
+        st = ServeStatus()
+        rc = self.lib.mps_serve_wait(self.sv, ticket, timeout, ctypes.byref(st))
+        if rc not in (MPS_OK, MPS_E_TIMEOUT):
+            raise MpsError(rc, f"ticket {ticket} failed")
+        return {k: getattr(st, k) for k, _ in ServeStatus._fields_} | {"done": rc == MPS_OK}
+
+    def result(self, ticket: int):
+        n = ctypes.c_size_t()
+        rc = self.lib.mps_serve_result(self.sv, ticket, None, 0, ctypes.byref(n))
+        if rc not in (MPS_OK, MPS_E_CAPACITY):
+            raise MpsError(rc, f"result {ticket}")
+        buf = (Relation * max(n.value, 1))()
+        rc = self.lib.mps_serve_result(self.sv, ticket, buf, n.value, ctypes.byref(n))
+        if rc != MPS_OK:
+            raise MpsError(rc, f"result {ticket}")
+        return [(buf[i].p, buf[i].M, buf[i].q) for i in range(n.value)]
+
+    def release(self, ticket: int):
+        self.lib.mps_serve_release(self.sv, ticket)
+
+    def checkpoint(self, ticket: int) -> tuple[int, int]:
+        a, b = ctypes.c_uint64(), ctypes.c_uint64()
+        rc = self.lib.mps_serve_checkpoint(self.sv, ticket, ctypes.byref(a), ctypes.byref(b))
+        if rc != MPS_OK:
+            raise MpsError(rc, "checkpoint")
+        return a.value, b.value
+
+    def close(self):
+        if self.sv:
+            self.lib.mps_serve_close(self.sv)
+            self.sv = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
