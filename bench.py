@@ -1,12 +1,16 @@
-"""Benchmark: sieved primes/s of the B200 siever on the plain full-size item.
+"""Benchmark: sieved primes/s of the B200 siever.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c2|c3|c1] [--width W] [--plain]
+                    [--workload c2|c3|c1|c4|c5] [--width W] [--plain]
 
-One step is one pass of the hot path (segment sieve -> prep -> exact BSGS ->
-order) over one item's whole P range, through the C-ABI (mps_item_relations).
-Default workload (the plain GPU path, full size): b=10, c=111,
-10^12 <= p < 10^12 + 10^10, 0 <= n < 10^7, n == 4 (mod 6).
+c1-c3: one step is one pass of the hot path (segment sieve -> prep -> exact
+BSGS -> order) over one item's whole P range, through the C-ABI
+(mps_item_relations).  Default workload (the plain GPU path, full size):
+b=10, c=111, 10^12 <= p < 10^12 + 10^10, 0 <= n < 10^7, n == 4 (mod 6).
+c4: one step is the 64-item mixed batch through mps_batch_relations (the
+batched engine); the plain per-item path is timed once beside it.
+c5: the served stream (mps_serve_*): Poisson arrivals at 0.5x-2x the measured
+batched capacity; p50/p99 item latency per rate.
 
 Under torchrun (N > 1) every rank sieves its own P slice of the same width
 (weak scaling, no data-path collective); the per-step time is the max over
@@ -39,6 +43,136 @@ WORKLOADS = {
            "small CPU-runnable: b=2 c=-25 p in [1e6, 1e8) n in [0, 1e5) n==1 mod 2"),
 }
 CPU_SAMPLE_WIDTH = {"c2": 30_000_000, "c3": 20_000_000, "c1": 99_000_000}
+
+
+def run_batch(args, siever_cls, make_item, workloads, rank, world, local, dist):
+    """c4: the mixed batch, batched engine vs the plain per-item path."""
+    import mps_b200
+    specs = workloads.c4_items(max_width=int(args.width) if args.width else None)
+    items = [make_item(*sp) for sp in specs]
+    with mps_b200.Siever(local) as counter:
+        nprimes = sum(counter.count_primes(sp[2], sp[3]) for sp in specs)
+    total_primes = sum_over_ranks(dist, local, float(nprimes))
+
+    def timed(siever, steps, warmup):
+        for _ in range(warmup):
+            siever.batch_relations(items)
+        dev, wall, launches, rels = 0.0, 0.0, 0, 0
+        bsgs_ms, bsgs_steps = 0.0, 0
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            r = siever.batch_relations(items)
+            wall += time.perf_counter() - t0
+            st = siever.stats()
+            dev += st["device_ms"] / 1e3
+            launches += st["kernel_launches"]
+            bsgs_ms += st["bsgs_ms"]
+            bsgs_steps += st["bsgs_steps"]
+            rels = len(r)
+        return dev, wall, launches, rels, bsgs_ms, bsgs_steps
+
+    batched = mps_b200.Siever(local)
+    clocks = ClockSampler(local)
+    barrier(dist, local)
+    clocks.start()
+    dev, wall, launches, rels, bsgs_ms, bsgs_steps = timed(batched, args.steps, args.warmup)
+    barrier(dist, local)
+    clk = clocks.stop()
+    peaks = batched.measure_peaks()
+    batched.close()
+    plain = mps_b200.Siever(local, plain=1, chunk_odds=1 << 23)
+    pdev, pwall, plaunches, prels, _, _ = timed(plain, 1, 1)
+    plain.close()
+    if prels != rels:
+        raise RuntimeError("plain and batched relation counts differ")
+    dev = max_over_ranks(dist, local, dev)
+    wall = max_over_ranks(dist, local, wall)
+    pdev = max_over_ranks(dist, local, pdev)
+    value = total_primes * args.steps / dev
+    if rank == 0:
+        mul_peak = peaks["fp64_mulmod_per_s"]
+        rate = bsgs_steps / (bsgs_ms / 1e3) if bsgs_ms else 0.0
+        line = {
+            "metric": "sieved primes/s", "value": value, "unit": "primes/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": f"mixed batch: 64 items seed {workloads.C4_SEED}" +
+                                   (f", P width capped at {args.width:.3g}" if args.width else ", full widths"),
+                       "path": "batched (multi-item waves, graph replay, two overlapped slots)",
+                       "l2": "working set per wave > 126 MB L2; no flush"},
+            "plain_per_item": {"value": total_primes / pdev, "unit": "primes/s", "ms_per_step": pdev * 1e3,
+                               "path": "one item after another, 2^23-odd chunks, host sync per stage",
+                               "kernel_launches": plaunches},
+            "e2e": {"value": total_primes * args.steps / wall, "unit": "primes/s",
+                    "h2d_bytes_per_step": 112 * len(items), "d2h_bytes_per_step": 28 * rels},
+            "gpu_launches": launches, "relations": rels, "primes": int(total_primes),
+            "roofline": {"bound": "fp64-pipe modular multiply", "kernel": "k_bsgs", "achieved": rate / 1e9,
+                         "peak": mul_peak / 1e9, "unit": "G mulmod/s", "frac": rate / mul_peak if mul_peak else None,
+                         "traffic": None, "note": "two slots overlap, so BSGS event time double-counts overlap"},
+            "cpu_baseline": None, "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_serve(args, rank):
+    """c5: Poisson arrivals of mixed items at multiples of the batched capacity."""
+    import mps_b200
+    import workloads
+    if rank != 0:
+        return 0
+    cap_w = int(args.width) if args.width else 10**9
+    duration = args.duration
+    # capacity: items/s of the batched engine on mixed items of the same distribution
+    probe = workloads.c4_items(n=32, seed=workloads.C4_SEED + 99, max_width=cap_w)
+    with mps_b200.Siever(0) as s:
+        s.batch_relations([mps_b200.make_item(*x) for x in probe])
+        t0 = time.perf_counter()
+        s.batch_relations([mps_b200.make_item(*x) for x in probe])
+        cap_items = len(probe) / (time.perf_counter() - t0)
+        nprimes_probe = sum(s.count_primes(x[2], x[3]) for x in probe)
+    results = []
+    clocks = ClockSampler(0)
+    clocks.start()
+    for mult in (0.5, 1.0, 1.5, 2.0):
+        rate = mult * cap_items
+        arrivals = workloads.c5_arrivals(rate, duration, max_width=cap_w)
+        lat, qms = [], []
+        with mps_b200.Server(0, max_active=256) as sv:
+            t_start = time.perf_counter()
+            tickets = []
+            for t_arr, spec in arrivals:
+                now = time.perf_counter() - t_start
+                if t_arr > now:
+                    time.sleep(t_arr - now)
+                tickets.append(sv.submit(mps_b200.make_item(*spec)))
+            for t in tickets:
+                st = sv.wait(t, timeout=3600)
+                lat.append(st["latency_ms"])
+                qms.append(st["queue_ms"])
+            span = time.perf_counter() - t_start
+        with mps_b200.Siever(0) as s:
+            nprimes = sum(s.count_primes(x[1][2], x[1][3]) for x in arrivals)
+        lat.sort()
+        pct = lambda q: lat[min(len(lat) - 1, int(q * len(lat)))] if lat else None
+        results.append({"load": mult, "arrival_rate_items_s": rate, "items": len(arrivals),
+                        "p50_ms": pct(0.50), "p99_ms": pct(0.99), "mean_queue_ms": statistics.mean(qms) if qms else None,
+                        "primes_per_s": nprimes / span, "makespan_s": span})
+    clk = clocks.stop()
+    best = max(r["primes_per_s"] for r in results)
+    line = {
+        "metric": "sieved primes/s (served) with p50/p99 item latency", "value": best, "unit": "primes/s",
+        "n_gpus": 1, "steps": len(results), "warmup": 1, "ms_per_step": None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": f"served stream: c4-distributed items, Poisson arrivals, {duration:.0f} s per rate "
+                               f"(600 s in the spec, shortened), P width capped at {cap_w:.3g}",
+                   "capacity_items_per_s": cap_items, "capacity_primes_per_s": nprimes_probe * cap_items / len(probe)},
+        "rates": results,
+        "e2e": {"value": best, "unit": "primes/s", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 def peaks_file():
@@ -196,11 +330,25 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + ["c4", "c5"])
+    ap.add_argument("--duration", type=float, default=15.0, help="c5: seconds of arrivals per rate")
     ap.add_argument("--width", type=float, default=None, help="P width per rank (default: the workload's)")
     ap.add_argument("--plain", action="store_true", help="the plain per-chunk path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.workload in ("c4", "c5"):
+        if args.impl == "reference":
+            spec = WORKLOADS["c2"]
+            return run_reference(args, spec, spec[-1])
+        rank, world, local, dist = dist_setup(args.gpus)
+        import mps_b200
+        import workloads
+        if args.workload == "c5":
+            return run_serve(args, rank)
+        rc = run_batch(args, mps_b200.Siever, mps_b200.make_item, workloads, rank, world, local, dist)
+        if dist is not None:
+            dist.destroy_process_group()
+        return rc
     spec = WORKLOADS[args.workload]
     b, c, P0, width, N0, N1, mod, res, label = spec
     if args.width is not None:

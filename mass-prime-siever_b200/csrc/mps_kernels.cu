@@ -1200,18 +1200,45 @@ __global__ void k_commit(const WaveDesc* w, const RawRelation* rel, const Counte
 
 // ------------------------------------------------------ prime counting --
 
+// Strong probable-prime test of p to base a (a < p) in field F.
+template <class F>
+__device__ __forceinline__ bool sprp_f(const F& f, u64 p, u64 a) {
+    const u64 pm1 = p - 1;
+    const int s = __ffsll((long long)pm1) - 1;
+    typename F::V x = f.pow(f.from_u64(a), pm1 >> s);
+    u64 y = f.residue(x);
+    if (y == 1 || y == pm1) return true;
+    for (int r = 1; r < s; ++r) {
+        x = f.mul(x, x);
+        y = f.residue(x);
+        if (y == pm1) return true;
+        if (y == 1) return false;
+    }
+    return false;
+}
+
+// Exact primality of an odd p > 37 with no factor <= 37: strong tests to the
+// 12 bases 2..37 (the set of is_prime64, Math.hpp:209-251), in field F.
+template <class F>
+__device__ bool is_prime_f(u64 p) {
+    const u32 bases[12] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37};
+    F f;
+    f.init(p);
+    for (int i = 0; i < 12; ++i)
+        if (!sprp_f(f, p, bases[i])) return false;
+    return true;
+}
+
 __global__ void __launch_bounds__(256) k_count_primes(const u64* surv, u64 surv_cap, Counters* ctr) {
     const u64 n = min((u64)*(volatile unsigned long long*)&ctr->survivors, surv_cap);
     u32 mine = 0;
     for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
         const u64 p = surv[i];
         bool prime;
-        if (p < 1000) {
+        if (p < 65536ull * 65536ull) {
             prime = true;                               // survivors below 65536^2 are the primes
         } else {
-            Mont M;
-            M.init(p);
-            prime = sprp2(M) && is_prime64(p);
+            prime = p < kFp64Limit ? is_prime_f<FieldF>(p) : is_prime_f<FieldM>(p);
         }
         mine += prime ? 1u : 0u;
     }

@@ -199,3 +199,8 @@ def test_argument_errors(siever, mps_lib):
         assert e.value.code == code, spec
     # the context stays usable
     assert siever.item_relations(item(mps_lib, (2, -25, 10**6, 10**6 + 100_000, 0, 1000, 1, 0))) is not None
+
+
+def test_prime_count_above_2_32(siever, oracle):
+    for lo in (10**12, 95 * 10**12, (1 << 52) + 7, (1 << 61)):
+        assert siever.count_primes(lo, lo + 300_000) == len(oracle.primes(lo, lo + 300_000, 1 << 16))
