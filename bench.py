@@ -43,6 +43,7 @@ WORKLOADS = {
            "small CPU-runnable: b=2 c=-25 p in [1e6, 1e8) n in [0, 1e5) n==1 mod 2"),
 }
 CPU_SAMPLE_WIDTH = {"c2": 30_000_000, "c3": 20_000_000, "c1": 99_000_000}
+ROOFLINE_WIDTH = 2 * 10**9          # P width of the k_bsgs roofline pass
 
 
 def run_batch(args, siever_cls, make_item, workloads, rank, world, local, dist):
@@ -89,9 +90,12 @@ def run_batch(args, siever_cls, make_item, workloads, rank, world, local, dist):
     wall = max_over_ranks(dist, local, wall)
     pdev = max_over_ranks(dist, local, pdev)
     value = total_primes * args.steps / dev
+    with mps_b200.Siever(local) as rs:
+        pieces = [(sp[2], min(sp[3], sp[2] + 10**8), make_item(*sp[:3], min(sp[3], sp[2] + 10**8), *sp[4:]))
+                  for sp in specs]
+        roofline = bsgs_roofline(rs, pieces, peaks, all(sp[3] <= (1 << 49) for sp in specs))
+    roofline["sample"] = "the first 1e8 of every item, one chunk per launch, one stream"
     if rank == 0:
-        mul_peak = peaks["fp64_mulmod_per_s"]
-        rate = bsgs_steps / (bsgs_ms / 1e3) if bsgs_ms else 0.0
         line = {
             "metric": "sieved primes/s", "value": value, "unit": "primes/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev * 1e3 / args.steps,
@@ -106,9 +110,7 @@ def run_batch(args, siever_cls, make_item, workloads, rank, world, local, dist):
             "e2e": {"value": total_primes * args.steps / wall, "unit": "primes/s",
                     "h2d_bytes_per_step": 112 * len(items), "d2h_bytes_per_step": 28 * rels},
             "gpu_launches": launches, "relations": rels, "primes": int(total_primes),
-            "roofline": {"bound": "fp64-pipe modular multiply", "kernel": "k_bsgs", "achieved": rate / 1e9,
-                         "peak": mul_peak / 1e9, "unit": "G mulmod/s", "frac": rate / mul_peak if mul_peak else None,
-                         "traffic": None, "note": "two slots overlap, so BSGS event time double-counts overlap"},
+            "roofline": roofline,
             "cpu_baseline": None, "clocks": clk,
         }
         print(json.dumps(line), flush=True)
@@ -173,6 +175,55 @@ def run_serve(args, rank):
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def profile_traffic(kernel: str):
+    """DRAM bytes per BSGS step of `kernel` from the committed ncu summary
+    (profiles/traffic.txt lines: "<kernel> <bytes per step> <source ...>")."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.txt")) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) >= 2 and parts[0] == kernel and not line.startswith("#"):
+                    return float(parts[1]), " ".join(parts[2:])
+    except OSError:
+        pass
+    return None, None
+
+
+def bsgs_roofline(siever, pieces, peaks, fp64_path: bool) -> dict:
+    """k_bsgs alone: the same persistent kernel launched one chunk at a time on
+    one stream (mps_chunk_relations), so its CUDA events time it without the
+    overlap of the two-slot engine.  achieved = BSGS steps (one modular
+    multiply and one table operation each, counted on the device) per second
+    of k_bsgs launch time; peak = the live-measured mulmod rate of the same
+    arithmetic without table work."""
+    steps, ms, launches, entries = 0, 0.0, 0, 0
+    for lo, hi, item in pieces:
+        siever.chunk_relations(lo, hi, item)
+        st = siever.stats()
+        steps += st["bsgs_steps"]
+        ms += st["bsgs_ms"]
+        launches += st["bsgs_launches"]
+        entries += st["entries"]
+    mul_peak = peaks["fp64_mulmod_per_s"] if fp64_path else peaks["int_mulmod_per_s"]
+    rate = steps / (ms / 1e3) if ms > 0 else 0.0
+    per_step, src = profile_traffic("k_bsgs")
+    steps_per_launch = steps / launches if launches else 0
+    hbm = peaks_file().get("hbm_gbs")
+    return {"bound": "alu (fp64-pipe modular multiply + shared-memory table)" if fp64_path
+            else "alu (int-pipe Montgomery multiply + shared-memory table)",
+            "kernel": "k_bsgs", "achieved": rate / 1e9, "peak": mul_peak / 1e9, "unit": "G mulmod/s",
+            "frac": rate / mul_peak if mul_peak else None,
+            "avg_launch_ms": ms / launches if launches else None, "steps_per_launch": steps_per_launch,
+            "traffic": per_step * steps_per_launch if per_step is not None else None,
+            "traffic_unit": "DRAM bytes per launch", "traffic_source": src,
+            "peak_source": "measured live (mps_measure_peaks): independent-chain mulmod probe, same arithmetic",
+            "peaks_measured": {k: v / 1e9 for k, v in peaks.items()},
+            "hbm_side": {"algorithmic_bytes_per_launch": 72.0 * entries / launches if launches else None,
+                         "note": "72 B entry read per prime; relations are a few bytes per launch",
+                         "frac_of_measured_hbm": (72.0 * entries / (ms / 1e3)) / (hbm * 1e9) if ms > 0 and hbm
+                         else None}}
 
 
 def peaks_file():
@@ -396,8 +447,10 @@ def main():
 
     peaks = siever.measure_peaks()
     fp64_path = hi <= (1 << 49)
-    mul_peak = peaks["fp64_mulmod_per_s"] if fp64_path else peaks["int_mulmod_per_s"]
-    bsgs_rate = steps_done / (bsgs_ms / 1e3) if bsgs_ms > 0 else 0.0
+    rw = min(width, ROOFLINE_WIDTH)
+    roofline = bsgs_roofline(siever, [(lo, lo + rw, mps_b200.make_item(b, c, lo, lo + rw, N0, N1, mod, res))],
+                             peaks, fp64_path)
+    roofline["sample"] = f"[P0, P0+{rw:.3g}) of this rank's slice, one chunk per launch, one stream"
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -419,11 +472,7 @@ def main():
                     "d2h_bytes_per_step": 24 * rel_count},
             "gpu_launches": launches,
             "relations": rel_count, "bsgs_primes": entries, "primes": int(total_primes),
-            "roofline": {"bound": "fp64-pipe modular multiply" if fp64_path else "int-pipe modular multiply",
-                         "kernel": "k_bsgs", "achieved": bsgs_rate / 1e9, "peak": mul_peak / 1e9,
-                         "unit": "G mulmod/s", "frac": bsgs_rate / mul_peak if mul_peak else None,
-                         "traffic": None, "peak_source": "measured live: independent-chain mulmod probe",
-                         "peaks_measured": {k: v / 1e9 for k, v in peaks.items()}},
+            "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clk,
         }

@@ -1434,9 +1434,17 @@ int mps_test_bsgs(mps_ctx* c, const uint64_t* cases, size_t count, uint32_t tabl
     u64* dj = nullptr;
     CK(cudaMalloc((void**)&dc, std::max<size_t>(count, 1) * 5 * sizeof(u64)), "alloc");
     CK(cudaMalloc((void**)&dj, std::max<size_t>(count, 1) * sizeof(u64)), "alloc");
+    std::memset(&c->stats, 0, sizeof(c->stats));
     cudaError_t e = cudaMemcpy(dc, cases, count * 5 * sizeof(u64), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaEventRecord(c->evb0, c->stream);
     if (e == cudaSuccess) e = launch_bsgs_direct(dc, dj, count, table_bits, c->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(c->evb1, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    float ms = 0;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, c->evb0, c->evb1);
+    c->stats.bsgs_ms = ms;
+    c->stats.bsgs_launches = 1;
+    c->stats.kernel_launches = 1;
     if (e == cudaSuccess) e = cudaMemcpy(j_out, dj, count * sizeof(u64), cudaMemcpyDeviceToHost);
     cudaFree(dc);
     cudaFree(dj);

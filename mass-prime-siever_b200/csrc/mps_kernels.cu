@@ -1329,7 +1329,7 @@ __global__ void k_bsgs_direct(const u64* cases, u64* j_out, u64 count, u32 tbits
         result = ~0ull;
     } else {
         u32 m = (u32)isqrt_ceil_dev(e.jcount);
-        const u32 cap = min(kMaxBaby, (1u << tbits) / 2);
+        const u32 cap = min(kMaxBaby, max(1u, (1u << tbits) / 5));      // the table load of the sieving path
         if (m > cap) m = cap;
         e.m = m;
         Mont M;

@@ -89,17 +89,19 @@ void write_progress(const WorkItem& it, i128 p_done) {
     if (std::rename(tmp.c_str(), kProgress) != 0) log_fatal(std::string("Failed to replace ") + kProgress);
 }
 
+// Core files are looked for at ids 0 .. kCoreScan - 1 (the reference stops at
+// the second missing id in a row, Worker.hpp:373-380; scanning the whole
+// range also finds the files of a reference run whose first workers wrote
+// nothing).
+constexpr int kCoreScan = 1024;
+
 // Worker.hpp:369-463 (reference resume), then the exact progress record when present.
 void read_checkpoint(WorkItem& item) {
     i128 new_p0 = item.P1;
     bool any = false;
-    for (int id = 0;; ++id) {
+    for (int id = 0; id < kCoreScan; ++id) {
         std::ifstream in(core_path(id));
-        if (!in) {
-            std::ifstream next(core_path(id + 1));
-            if (!next) break;
-            continue;
-        }
+        if (!in) continue;
         std::string line, last;
         while (std::getline(in, line))
             if (!line.empty()) last = line;
@@ -128,13 +130,9 @@ void read_checkpoint(WorkItem& item) {
     }
     item.P0 = new_p0;
     uint64_t restored = 0;
-    for (int id = 0;; ++id) {
+    for (int id = 0; id < kCoreScan; ++id) {
         std::ifstream in(core_path(id));
-        if (!in) {
-            std::ifstream next(core_path(id + 1));
-            if (!next) break;
-            continue;
-        }
+        if (!in) continue;
         std::vector<std::string> kept;
         std::string line;
         while (std::getline(in, line)) {
@@ -155,19 +153,32 @@ void read_checkpoint(WorkItem& item) {
              ", relations restored = " + std::to_string(restored));
 }
 
-// Worker.hpp:469-495
-void merge_core_files(int ids) {
+// Worker.hpp:469-495, except that the lines are written in increasing p
+// (the reference concatenates the files, an order that depends on thread
+// timing), so relations.p is the same file on every run.
+void merge_core_files() {
+    std::vector<std::pair<unsigned long long, std::string>> lines;
+    for (int id = 0; id < kCoreScan; ++id) {
+        std::ifstream core(core_path(id));
+        if (!core) continue;
+        std::string line;
+        while (std::getline(core, line)) {
+            if (line.empty()) continue;
+            std::stringstream ss(line);
+            unsigned long long p = 0;
+            ss >> p;
+            lines.emplace_back(p, line);
+        }
+    }
+    std::stable_sort(lines.begin(), lines.end(),
+                     [](const auto& a, const auto& b) { return a.first < b.first; });
     std::ofstream merged("relations.p", std::ios::binary | std::ios::trunc);
     if (!merged) log_fatal("Failed to create relations.p");
-    for (int id = 0; id < ids + 64; ++id) {
-        std::ifstream core(core_path(id), std::ios::binary);
-        if (!core) continue;
-        merged << core.rdbuf();
-    }
+    for (const auto& l : lines) merged << l.second << '\n';
     merged.flush();
     if (!merged) log_fatal("Failed while writing relations.p");
     merged.close();
-    for (int id = 0; id < ids + 64; ++id) std::remove(core_path(id).c_str());
+    for (int id = 0; id < kCoreScan; ++id) std::remove(core_path(id).c_str());
 }
 
 std::string eta_text(std::chrono::steady_clock::time_point start, size_t done, size_t total) {
@@ -242,7 +253,7 @@ int main(int argc, char** argv) {
     log_info("GPU enabled (B200 sm_100a): device " + std::to_string(cfg.gpu_device) + ", libmps_b200 ABI " +
              std::to_string(mps_abi_version()));
 
-    const int worker_id = std::max(0, cfg.cpu_count);            // the reference's first GPU feeder id
+    const int worker_id = 0;                  // one writer: core_0.p, the first file any resume looks at
     const uint64_t ref_chunk = (uint64_t)cfg.memory_allowed_mb * 1024ull * 1024ull / (uint64_t)std::max(1, cfg.cpu_count);
     const uint64_t chunk = std::min<uint64_t>(std::max<uint64_t>(ref_chunk, 1ull << 24), 1ull << 32);
 
@@ -304,14 +315,13 @@ int main(int argc, char** argv) {
             break;
         }
         log_info("Merging core files");
-        merge_core_files(cfg.cpu_count + cfg.gpu_threads);
+        merge_core_files();
         const std::vector<Relation> rel = load_relations("relations.p");
         log_info("Loaded " + std::to_string(rel.size()) + " relation(s)");
         const auto cand = apply_relations(item, rel);
         append_results_json("results.json", results_entry(item, cand, now_timestamp()));
         log_info(final_status(item, cand, std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count()));
         log_info("Finished work item " + std::to_string(wi + 1));
-        for (int id = 0; id < cfg.cpu_count + cfg.gpu_threads + 64; ++id) std::remove(core_path(id).c_str());
         std::remove(kProgress);
     }
     if (!g_shutdown.load())
