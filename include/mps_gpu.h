@@ -63,12 +63,17 @@ typedef struct mps_tuning {
     uint32_t struct_size;       /* sizeof(mps_tuning)                                          */
     uint32_t table_bits;        /* baby-step table of 2^bits slots per prime (0: per item)     */
     uint64_t chunk_odds;        /* odd integers per device chunk (0: 2^26)                      */
-    uint32_t max_baby;          /* cap on the baby-step count (0: half the table)              */
+    uint32_t max_baby;          /* cap on the baby-step count (0: what the table holds)        */
     uint32_t bsgs_warps;        /* warps per BSGS block (0: 4)                                 */
-    uint32_t class_modulus;     /* Q of the power-residue split g = gcd(Q, p-1) (0: lcm(mod,24)) */
+    uint32_t class_modulus;     /* Q of the power-residue split g = gcd(Q, p-1)
+                                   (0: lcm(mod, 5040), or 5040 when that exceeds 100800)       */
     uint32_t full_mr;           /* 1: 12-base Miller-Rabin on every filter survivor (eager)    */
     uint32_t plain;             /* 1: plain per-chunk path (host sync between stages)          */
-    uint32_t reserved[7];
+    uint32_t chains;            /* BSGS chains per lane, 1, 2 or 4 (0: 2)                      */
+    uint32_t graphs_off;        /* 1: launch waves directly instead of replaying CUDA graphs   */
+    uint32_t table_kind;        /* BSGS table: 0 = four 16-bit fingerprints per 64-bit word,
+                                   1 = one 32-bit key per slot                                 */
+    uint32_t reserved[4];
 } mps_tuning;
 
 /* Counters of the last call (all chunks of it). */

@@ -168,20 +168,26 @@ int ensure_rel(mps_ctx* c, u64 need) {
     return MPS_OK;
 }
 
-// Baby-step table size for the item.  Every prime's j-range is at most K;
-// the table load is kept near 1/5 (a probe then reads one slot) and at most
-// 2^12 slots (8-16 KB per warp keeps ~24 warps resident per SM), so wide N
-// ranges trade baby steps for giant steps.
+// Baby-step table size for the item: 4 << tbits bytes per warp, at most
+// 8 KB by default (keeps ~24 warps resident per SM).  Every prime's j-range
+// is at most K, so m_opt = ceil(sqrt(K)) baby steps balance the giant steps;
+// a wider N range than the table holds trades baby steps for giant steps.
+// Fingerprint table (table_kind 0): 2^(tbits-1) words of four keys, filled
+// to at most one key per word on average.  32-bit slots (table_kind 1):
+// 2^tbits slots, load at most 1/5 (a probe then reads one slot).
 void table_for(const mps_ctx* c, u64 K, u32* tbits, u32* max_baby) {
     const u64 m_opt = (u64)std::ceil(std::sqrt((double)std::max<u64>(K, 1)));
+    const bool quad = c->tun.table_kind == 0;
+    const auto holds = [&](u32 tb) { return quad ? (1u << (tb - 1)) : std::max<u32>((1u << tb) / 5, 1); };
     u32 tb = c->tun.table_bits;
     if (tb == 0) {
         tb = 6;
-        while ((1ull << tb) < 5 * m_opt && tb < 11) ++tb;
+        while (holds(tb) < m_opt && tb < 11) ++tb;
     }
-    tb = std::min<u32>(std::max<u32>(tb, 5), 14);
-    u32 mb = c->tun.max_baby ? c->tun.max_baby : std::max<u32>((1u << tb) / 5, 1);
-    mb = std::min<u32>(std::min<u32>(mb, kMaxBaby), (1u << tb) - 1);
+    tb = std::min<u32>(std::max<u32>(tb, 6), 14);
+    u32 mb = c->tun.max_baby ? c->tun.max_baby : holds(tb);
+    const u32 cap = quad ? (1u << tb) : (1u << tb) - 1;       // fingerprints: at most two keys per word
+    mb = std::min<u32>(std::min<u32>(mb, kMaxBaby), cap);
     *tbits = tb;
     *max_baby = std::max<u32>(mb, 1);
 }
@@ -329,7 +335,8 @@ int run_chunk(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, std::vector<RawRelati
     ba.rel_cap = c->rel_cap;
     ba.tbits = tbits;
     ba.warps_per_block = warps;
-    ba.chains = c->tun.reserved[0] ? c->tun.reserved[0] : 2;
+    ba.chains = c->tun.chains ? c->tun.chains : 2;
+    ba.table_kind = c->tun.table_kind;
     ba.max_p = hi;
 
     OrderArgs oa{};
@@ -473,7 +480,8 @@ int slot_enqueue(mps_ctx* c, WaveSlot& w, u32 tbits, bool capturing) {
     pa.full_mr = c->tun.full_mr;
     BsgsArgs ba{};
     ba.ent = w.d_ent; ba.ent_cap = w.ent_cap; ba.rel = w.d_rel; ba.rel_cap = w.rel_cap; ba.tbits = tbits;
-    ba.warps_per_block = warps; ba.persistent = 1; ba.chains = c->tun.reserved[0] ? c->tun.reserved[0] : 2;
+    ba.warps_per_block = warps; ba.persistent = 1; ba.chains = c->tun.chains ? c->tun.chains : 2;
+    ba.table_kind = c->tun.table_kind;
     ba.max_p = 0;   // per-entry arithmetic
     OrderArgs oa{};
     oa.rel = w.d_rel; oa.rel_cap = w.rel_cap; oa.items = c->d_items; oa.tables = c->tables();
@@ -498,7 +506,7 @@ int slot_enqueue(mps_ctx* c, WaveSlot& w, u32 tbits, bool capturing) {
 }
 
 int slot_launch(mps_ctx* c, WaveSlot& w, u32 tbits) {
-    if (c->tun.reserved[1]) return slot_enqueue(c, w, tbits, false);       // graphs off (tuning)
+    if (c->tun.graphs_off) return slot_enqueue(c, w, tbits, false);
     if (!w.graph || w.graph_tbits != tbits || w.graph_items != c->d_items || w.graph_state != c->d_state) {
         if (w.graph) cudaGraphExecDestroy(w.graph);
         w.graph = nullptr;
@@ -1095,7 +1103,7 @@ int mps_filter(mps_ctx* c, const uint64_t* primes, size_t n, const mps_item* ite
         pa.ent = c->d_ent; pa.ent_cap = c->ent_cap; pa.rel = c->d_rel; pa.rel_cap = c->rel_cap; pa.full_mr = c->tun.full_mr;
         BsgsArgs ba{};
         ba.ent = c->d_ent; ba.ent_cap = c->ent_cap; ba.rel = c->d_rel; ba.rel_cap = c->rel_cap;
-        ba.tbits = tbits; ba.warps_per_block = warps; ba.persistent = 1; ba.chains = 2;
+        ba.tbits = tbits; ba.warps_per_block = warps; ba.persistent = 1; ba.chains = 2; ba.table_kind = c->tun.table_kind;
         ba.max_p = *std::max_element(primes + off, primes + off + cnt);
         OrderArgs oa{};
         oa.rel = c->d_rel; oa.rel_cap = c->rel_cap; oa.items = c->d_items; oa.tables = c->tables();
@@ -1437,7 +1445,7 @@ int mps_test_bsgs(mps_ctx* c, const uint64_t* cases, size_t count, uint32_t tabl
     std::memset(&c->stats, 0, sizeof(c->stats));
     cudaError_t e = cudaMemcpy(dc, cases, count * 5 * sizeof(u64), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaEventRecord(c->evb0, c->stream);
-    if (e == cudaSuccess) e = launch_bsgs_direct(dc, dj, count, table_bits, c->stream);
+    if (e == cudaSuccess) e = launch_bsgs_direct(dc, dj, count, table_bits, c->tun.table_kind, c->stream);
     if (e == cudaSuccess) e = cudaEventRecord(c->evb1, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     float ms = 0;

@@ -985,15 +985,218 @@ __device__ u64 solve_fp64(const Entry& e, u32* tab, u32 tbits, u64* steps_out) {
     return best < e.jcount ? best : ~0ull;
 }
 
+// ---- the FP64 solve with a fingerprint table (the default) ----
+//
+// Table: 2^tw 64-bit words per warp, each holding up to four 16-bit halves
+// filled in order (half k = bits 16k..16k+15): bit 15 of a half marks it
+// used, bits 0..13 hold a 14-bit fingerprint of the key; bit 14 of half 0 is
+// the word's overflow bit, set when a key homed at this word found it full
+// and moved on (linear probing over words).  The home word is the top tw bits
+// of the key's multiplicative hash h, the fingerprint the next 14 bits.  For
+// m baby steps tw = ceil(log2 m), so a word holds 0.5..1 keys on average and
+// fewer than 0.4% of the words overflow.  A probe reads one word and tests the
+// four halves at once (x = word ^ pattern has a zero 16-bit half exactly when
+// a half matches: (x - 0x0001..) & ~x & 0x8000.. is then nonzero); a home
+// with its overflow bit set also counts as a candidate.  Candidates leave the
+// hot loop: the lane walks the overflow chain, and a fingerprint found is
+// resolved exactly by recomputation (ffind_baby).  Compared with one 32-bit
+// key per slot this stores 2.5x as many baby steps in the same shared memory
+// and never walks inside the hot loop.
+
+constexpr u64 kQValid = 0x8000800080008000ull;
+constexpr u32 kQOvf = 0x4000u;
+
+__device__ __forceinline__ u32 fq_pattern(u32 h, u32 tw) {
+    return ((h >> (18 - tw)) & 0x3FFFu) | 0x8000u;
+}
+
+// Nonzero when a used half of (lo, hi) equals pat, or the word overflowed.
+__device__ __forceinline__ u32 fq_candidate(u32 lo, u32 hi, u32 pat) {
+    const u32 rep = pat * 0x10001u;
+    const u32 x0 = (lo & ~kQOvf) ^ rep, x1 = hi ^ rep;
+    const u32 z = ((x0 - 0x10001u) & ~x0) | ((x1 - 0x10001u) & ~x1);
+    return (z & 0x80008000u) | (lo & kQOvf);
+}
+
+__device__ __forceinline__ bool fq_word_has(u64 w, u32 pat) {
+    const u32 lo = (u32)w & ~kQOvf, hi = (u32)(w >> 32);
+    return (lo & 0xFFFFu) == pat || (lo >> 16) == pat || (hi & 0xFFFFu) == pat || (hi >> 16) == pat;
+}
+
+__device__ __forceinline__ void fq_insert(unsigned long long* tab, u32 mask, u32 home, u32 pat) {
+    volatile unsigned long long* vt = tab;
+    u32 s = home;
+    unsigned long long w = vt[s];
+    for (;;) {
+        if (w >> 63) {                               // full: move on (marking the home once)
+            if (s == home && !(w & kQOvf)) atomicOr(&tab[home], (unsigned long long)kQOvf);
+            s = (s + 1) & mask;
+            w = vt[s];
+            continue;
+        }
+        const u32 k = __popcll(w & kQValid);
+        const unsigned long long nw = w | ((unsigned long long)pat << (16 * k));
+        const unsigned long long old = atomicCAS(&tab[s], w, nw);
+        if (old == w) return;
+        w = old;
+    }
+}
+
+// Whether the key (home, pat) is in the table: its home word, then the
+// overflow chain up to the first word that is not full.
+__device__ __forceinline__ bool fq_contains(const unsigned long long* tab, u32 mask, u32 home, u32 pat) {
+    u64 w = tab[home];
+    if (fq_word_has(w, pat)) return true;
+    if (!(w & kQOvf)) return false;
+    for (u32 s = (home + 1) & mask, n = 0; n <= mask; s = (s + 1) & mask, ++n) {
+        w = tab[s];
+        if (fq_word_has(w, pat)) return true;
+        if (!(w >> 63)) return false;
+    }
+    return false;
+}
+
 template <int CH>
+__device__ u64 solve_fp64q(const Entry& e, unsigned long long* tab, u32 tbits, u64* steps_out) {
+    const u32 lane = threadIdx.x & 31;
+    Fp64 f;
+    f.init(e.p);
+    const u32 m = e.m;
+    const u32 jc = (u32)e.jcount;                      // jcount <= 10^7
+    // 2^tw words for m keys (0.5..1 per word), within the launch's 2^(tbits-1) words
+    const u32 tw = min(tbits - 1, max(5u, 32u - __clz(max(m, 2u) - 1)));
+    const u32 mask = (1u << tw) - 1, shift = 32 - tw;
+    const double B = (double)e.B, Bm = (double)e.Bm, tv = (double)e.t, G0 = (double)e.G0;
+
+    double xb = B, xg = Bm;                            // B^(l+1), Bm^(l+1)
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const double yb = __shfl_up_sync(FULL, xb, off), yg = __shfl_up_sync(FULL, xg, off);
+        if (lane >= (u32)off) {
+            xb = f.mul(xb, yb);
+            xg = f.mul(xg, yg);
+        }
+    }
+    const double B32 = __shfl_sync(FULL, xb, 31), Bm32 = __shfl_sync(FULL, xg, 31);
+    double bl = __shfl_up_sync(FULL, xb, 1);
+    if (lane == 0) bl = 1.0;
+    double Bstep = B32, Gstep = Bm32;                  // B^(32 CH), Bm^(32 CH)
+#pragma unroll
+    for (int c = 1; c < CH; c <<= 1) {
+        Bstep = f.mul(Bstep, Bstep);
+        Gstep = f.mul(Gstep, Gstep);
+    }
+    const double tbl = f.mul(tv, bl);
+    double bx[CH], gx[CH];
+    bx[0] = tbl;
+    gx[0] = f.mul(G0, xg);
+#pragma unroll
+    for (int c = 1; c < CH; ++c) {
+        bx[c] = f.mul(bx[c - 1], B32);
+        gx[c] = f.mul(gx[c - 1], Bm32);
+    }
+
+    uint4* t4 = reinterpret_cast<uint4*>(tab);
+    for (u32 k = lane; k <= mask / 2; k += 32) t4[k] = make_uint4(0, 0, 0, 0);
+    __syncwarp();
+
+    // baby steps, stopping at a cycle B^d == 1 (d < m)
+    u32 cyc = 0, baby_done = m;
+    for (u32 base = 0; base < m; base += 32 * CH) {
+        double cv[CH];
+        u32 cb = 0;
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            cv[c] = f.canon(bx[c]);
+            const u32 i = base + 32 * c + lane;
+            const u32 bc = __ballot_sync(FULL, i > 0 && i < m && cv[c] == tv);
+            if (bc && !cb) cb = base + 32 * c + __ffs(bc) - 1;
+        }
+        const u32 lim = cb ? cb : m;
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            const u32 i = base + 32 * c + lane;
+            if (i < lim) {
+                const u32 h = fhash(cv[c]);
+                fq_insert(tab, mask, h >> shift, fq_pattern(h, tw));
+            }
+        }
+        if (cb) {
+            cyc = cb;
+            baby_done = cb;
+            break;
+        }
+#pragma unroll
+        for (int c = 0; c < CH; ++c) bx[c] = f.mul(bx[c], Bstep);
+    }
+    __syncwarp();
+
+    u64 best = ~0ull;
+    u32 giant_done = 0;
+    if (cyc) {
+        const int i = ffind_baby(f, tbl, B32, 1, cyc, G0);
+        if (i > 0) best = cyc - (u32)i;
+    } else {
+        const u32 G = (jc - 1 + m - 1) / m;            // g = 1..G covers j in [1, G*m]
+        giant_done = G;
+        const uint2* t2 = reinterpret_cast<const uint2*>(tab);
+        for (u32 base = 0; base < G; base += 32 * CH) {
+            double cv[CH];
+            u32 hs[CH];
+            u32 cand = 0;
+#pragma unroll
+            for (int c = 0; c < CH; ++c) {
+                cv[c] = f.canon(gx[c]);
+                hs[c] = fhash(cv[c]);
+                const uint2 w = t2[hs[c] >> shift];
+                cand |= fq_candidate(w.x, w.y, fq_pattern(hs[c], tw)) ? (1u << c) : 0u;
+            }
+            if (__any_sync(FULL, cand)) {
+                // the rare path: walk overflowed homes, then resolve exact matches in increasing g
+                u32 real = 0;
+#pragma unroll
+                for (int c = 0; c < CH; ++c)
+                    if (((cand >> c) & 1u) && base + 32 * c + lane + 1 <= G &&
+                        fq_contains(tab, mask, hs[c] >> shift, fq_pattern(hs[c], tw)))
+                        real |= 1u << c;
+                u64 jb = ~0ull;
+#pragma unroll
+                for (int c = 0; c < CH; ++c) {
+                    u32 bb = __ballot_sync(FULL, (real >> c) & 1u);
+                    while (bb && jb == ~0ull) {
+                        const int src = __ffs(bb) - 1;
+                        bb &= bb - 1;
+                        const double v = __shfl_sync(FULL, cv[c], src);
+                        const u64 g = base + 32 * c + (u32)src + 1;
+                        const int i = ffind_baby(f, tbl, B32, 0, m, v);
+                        if (i >= 0) jb = g * m - (u64)i;
+                    }
+                }
+                if (jb != ~0ull) {
+                    best = jb;
+                    giant_done = min(G, base + 32 * CH);
+                    break;
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < CH; ++c) gx[c] = f.mul(gx[c], Gstep);
+        }
+    }
+    __syncwarp();
+    if (steps_out) *steps_out = (u64)baby_done + giant_done;
+    return best < e.jcount ? best : ~0ull;
+}
+
+template <int CH, int QT>
 __device__ __forceinline__ u64 solve_any(const Entry& e, void* tab, u32 tbits, u64* steps) {
     if (CH == 0 || e.p >= kFp64Limit) return solve_entry<FieldM>(e, (unsigned short*)tab, tbits + 1, steps);
+    if (QT == 0) return solve_fp64q<CH ? CH : 1>(e, (unsigned long long*)tab, tbits, steps);
     return solve_fp64<CH ? CH : 1>(e, (u32*)tab, tbits, steps);
 }
 
 // CH > 0: every entry has p < 2^49 (FP64 solve with CH chains per lane);
 // CH == 0: any p (integer Montgomery solve).
-template <int CH>
+template <int CH, int QT>
 __global__ void __launch_bounds__(256, MPS_BSGS_MINB) k_bsgs(BsgsArgs a, Counters* ctr) {
     extern __shared__ __align__(16) u32 smem32[];
     const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1008,7 +1211,7 @@ __global__ void __launch_bounds__(256, MPS_BSGS_MINB) k_bsgs(BsgsArgs a, Counter
             if (idx >= n_ent) break;
             const Entry e = a.ent[idx];
             u64 steps = 0;
-            const u64 j = solve_any<CH>(e, tab, a.tbits, &steps);
+            const u64 j = solve_any<CH, QT>(e, tab, a.tbits, &steps);
             if (lane == 0) {
                 if (j != ~0ull) emit_relation(e.p, e.n_first + j * e.L, 0, e.item, a.rel, a.rel_cap, ctr);
                 my_steps += steps;
@@ -1020,7 +1223,7 @@ __global__ void __launch_bounds__(256, MPS_BSGS_MINB) k_bsgs(BsgsArgs a, Counter
         if (idx >= n_ent) return;
         const Entry e = a.ent[idx];
         u64 steps = 0;
-        const u64 j = solve_any<CH>(e, tab, a.tbits, &steps);
+        const u64 j = solve_any<CH, QT>(e, tab, a.tbits, &steps);
         if (lane == 0) {
             if (j != ~0ull) emit_relation(e.p, e.n_first + j * e.L, 0, e.item, a.rel, a.rel_cap, ctr);
             atomicAdd(&ctr->steps, (unsigned long long)steps);
@@ -1311,7 +1514,7 @@ __global__ void k_is_prime(const u64* n, u32* out, u64 count) {
 }
 
 // cases[5i..5i+4] = p, B, G0, t, jcount (plain residues); one warp per case.
-__global__ void k_bsgs_direct(const u64* cases, u64* j_out, u64 count, u32 tbits) {
+__global__ void k_bsgs_direct(const u64* cases, u64* j_out, u64 count, u32 tbits, u32 table_kind) {
     extern __shared__ __align__(16) u32 smem32[];
     const u64 idx = blockIdx.x;
     if (idx >= count) return;
@@ -1329,14 +1532,17 @@ __global__ void k_bsgs_direct(const u64* cases, u64* j_out, u64 count, u32 tbits
         result = ~0ull;
     } else {
         u32 m = (u32)isqrt_ceil_dev(e.jcount);
-        const u32 cap = min(kMaxBaby, max(1u, (1u << tbits) / 5));      // the table load of the sieving path
+        // the table loads of the sieving path
+        const u32 cap = min(kMaxBaby, table_kind == 0 ? 1u << (tbits - 1) : max(1u, (1u << tbits) / 5));
         if (m > cap) m = cap;
         e.m = m;
         Mont M;
         M.init(p);
         const u64 rr = M.r2();
         e.Bm = M.from_mont(M.pow(M.to_mont(e.B, rr), m));
-        result = e.p < kFp64Limit ? solve_any<2>(e, smem32, tbits, nullptr) : solve_any<0>(e, smem32, tbits, nullptr);
+        if (e.p >= kFp64Limit) result = solve_any<0, 0>(e, smem32, tbits, nullptr);
+        else if (table_kind == 0) result = solve_any<2, 0>(e, smem32, tbits, nullptr);
+        else result = solve_any<2, 1>(e, smem32, tbits, nullptr);
     }
     if (threadIdx.x == 0) j_out[idx] = result;
 }
@@ -1380,7 +1586,8 @@ cudaError_t launch_prep(const PrepArgs& a, Counters* ctr, int grid, cudaStream_t
 cudaError_t bsgs_reserve_smem(size_t smem) {
     static size_t done = 0;
     if (smem <= done) return cudaSuccess;
-    for (auto kern : {k_bsgs<0>, k_bsgs<1>, k_bsgs<2>, k_bsgs<4>}) {
+    for (auto kern : {k_bsgs<0, 0>, k_bsgs<1, 0>, k_bsgs<2, 0>, k_bsgs<4, 0>, k_bsgs<1, 1>, k_bsgs<2, 1>,
+                      k_bsgs<4, 1>}) {
         cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (err != cudaSuccess) return err;
     }
@@ -1396,10 +1603,15 @@ cudaError_t launch_bsgs(const BsgsArgs& a, Counters* ctr, int grid, cudaStream_t
         kern<<<grid, a.warps_per_block * 32, smem, s>>>(a, ctr);
         return cudaGetLastError();
     };
-    if (a.max_p >= kFp64Limit) return go(k_bsgs<0>);
-    if (a.chains == 4) return go(k_bsgs<4>);
-    if (a.chains == 1) return go(k_bsgs<1>);
-    return go(k_bsgs<2>);
+    if (a.max_p >= kFp64Limit) return go(k_bsgs<0, 0>);
+    if (a.table_kind == 1) {
+        if (a.chains == 4) return go(k_bsgs<4, 1>);
+        if (a.chains == 1) return go(k_bsgs<1, 1>);
+        return go(k_bsgs<2, 1>);
+    }
+    if (a.chains == 4) return go(k_bsgs<4, 0>);
+    if (a.chains == 1) return go(k_bsgs<1, 0>);
+    return go(k_bsgs<2, 0>);
 }
 
 cudaError_t launch_order(const OrderArgs& a, Counters* ctr, int grid, cudaStream_t s) {
@@ -1439,12 +1651,12 @@ cudaError_t launch_is_prime(const u64* n, u32* out, u64 count, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_bsgs_direct(const u64* cases, u64* j_out, u64 count, u32 tbits, cudaStream_t s) {
+cudaError_t launch_bsgs_direct(const u64* cases, u64* j_out, u64 count, u32 tbits, u32 table_kind, cudaStream_t s) {
     if (count == 0) return cudaSuccess;
     const size_t smem = (size_t)4 << tbits;
     cudaError_t err = cudaFuncSetAttribute(k_bsgs_direct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
-    k_bsgs_direct<<<(unsigned)count, 32, smem, s>>>(cases, j_out, count, tbits);
+    k_bsgs_direct<<<(unsigned)count, 32, smem, s>>>(cases, j_out, count, tbits, table_kind);
     return cudaGetLastError();
 }
 

@@ -88,6 +88,7 @@ struct BsgsArgs {
     u32 persistent;            // 1: work-stealing warps; 0: one warp per entry
     u32 chains;                // FP64 solve: independent chains per lane (1, 2, 4)
     u64 max_p;                 // largest p of the entries (>= 2^49: integer solve)
+    u32 table_kind;            // FP64 solve: 0 = fingerprint words, 1 = 32-bit slots
 };
 cudaError_t launch_bsgs(const BsgsArgs& a, Counters* ctr, int grid, cudaStream_t s);
 cudaError_t bsgs_reserve_smem(size_t smem);   // call before capturing a launch_bsgs
@@ -112,7 +113,7 @@ cudaError_t launch_fmul_peak(u64 p, u32 iters, int grid, u64* sink, cudaStream_t
 // Test hooks: raw kernels on given inputs.
 cudaError_t launch_is_prime(const u64* n, u32* out, u64 count, cudaStream_t s);
 cudaError_t launch_bsgs_direct(const u64* cases /* p,B,G0,t,jcount */, u64* j_out, u64 count, u32 tbits,
-                               cudaStream_t s);
+                               u32 table_kind, cudaStream_t s);
 cudaError_t launch_order_direct(const u64* bp /* b,p pairs */, u64* q_out, u64 count, SieveTables t,
                                 cudaStream_t s);
 

@@ -48,7 +48,8 @@ class Tuning(ctypes.Structure):
         ("chunk_odds", ctypes.c_uint64), ("max_baby", ctypes.c_uint32),
         ("bsgs_warps", ctypes.c_uint32), ("class_modulus", ctypes.c_uint32),
         ("full_mr", ctypes.c_uint32), ("plain", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 7),
+        ("chains", ctypes.c_uint32), ("graphs_off", ctypes.c_uint32), ("table_kind", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 4),
     ]
 
 

@@ -68,10 +68,12 @@ def _bsgs_cases(seed, count):
     return cases
 
 
-@pytest.mark.parametrize("table_bits", [6, 9, 12, 13])
-def test_bsgs_smallest_j(siever, oracle, table_bits):
+@pytest.mark.parametrize("table_bits", [5, 6, 9, 12, 13])
+@pytest.mark.parametrize("table_kind", [0, 1])
+def test_bsgs_smallest_j(mps_lib, oracle, table_bits, table_kind):
     cases = _bsgs_cases(100 + table_bits, 400)
-    got = siever.bsgs(cases, table_bits=table_bits)
+    with mps_lib.Siever(0, table_kind=table_kind) as s:
+        got = s.bsgs(cases, table_bits=table_bits)
     want = [oracle.bsgs_smallest_j(*c) for c in cases]
     bad = [(c, g, w) for c, g, w in zip(cases, got, want) if g != w]
     assert not bad, bad[:3]
@@ -121,7 +123,8 @@ def test_c1_prime_count(siever, golden):
 @pytest.mark.parametrize("tuning", [
     dict(plain=1), dict(full_mr=1), dict(table_bits=6), dict(table_bits=9, max_baby=100),
     dict(class_modulus=2), dict(class_modulus=48), dict(class_modulus=720), dict(chunk_odds=40_000),
-    dict(bsgs_warps=1), dict(bsgs_warps=8, table_bits=11),
+    dict(bsgs_warps=1), dict(bsgs_warps=8, table_bits=11), dict(table_kind=1), dict(table_kind=1, chains=4),
+    dict(chains=1), dict(chains=4), dict(table_bits=7, max_baby=256), dict(graphs_off=1),
 ])
 def test_tunings_give_identical_relations(mps_lib, oracle, tuning):
     specs = [(2, -25, 10**10, 10**10 + 4_000_000, 3_600_000, 5_000_000, 2, 1),

@@ -274,7 +274,7 @@ def test_resume_reference_checkpoint(siever_bin, tmp_path, oracle):
     record): resume at the smallest last p, as the reference does."""
     from oracle.oracle import make_item as oracle_item
 
-    item = (10, 111, 10**12, 10**12 + 5 * 10**7, 0, 10**7, 6, 4)
+    item = (2, -25, 10**9, 10**9 + 10**8, 0, 100_000, 2, 1)
     want = oracle.relations(item[2], item[3], oracle_item(*item))
     assert len(want) > 40
     _write_job(tmp_path, [item], cpu=2)
