@@ -63,6 +63,14 @@ def shard_bounds(P0: int, P1: int, world: int, rank: int) -> tuple[int, int]:
     return lo, hi
 
 
+def slice_relations(compute, spec: tuple, world: int, rank: int) -> list[tuple[int, int, int]]:
+    """This rank's relations: compute(lo, hi, spec) on its slice, or [] when
+    the slice is empty (a P range narrower than the world size), so that
+    every rank still reaches the gather."""
+    lo, hi = shard_bounds(spec[2], spec[3], world, rank)
+    return compute(lo, hi, spec) if lo < hi else []
+
+
 def merge_relations(parts: list[list[tuple[int, int, int]]]) -> list[tuple[int, int, int]]:
     """Concatenate per-rank relations (disjoint P slices) in increasing p."""
     out = sorted(r for part in parts for r in part)
@@ -131,11 +139,14 @@ def main(argv=None) -> int:
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     import mps_b200
-    b, c, P0, P1, N0, N1, mod, res = spec
-    lo, hi = shard_bounds(P0, P1, world, rank)
+
+    def on_gpu(lo, hi, sp):
+        b, c, _, _, N0, N1, mod, res = sp
+        with mps_b200.Siever(local) as s:
+            return s.item_relations(mps_b200.make_item(b, c, lo, hi, N0, N1, mod, res))
+
     t0 = time.perf_counter()
-    with mps_b200.Siever(local) as s:
-        rels = s.item_relations(mps_b200.make_item(b, c, lo, hi, N0, N1, mod, res))
+    rels = slice_relations(on_gpu, spec, world, rank)
     dt = time.perf_counter() - t0
     merged = gather_relations(dist, rels, rank, world)
     if rank == 0:

@@ -15,17 +15,28 @@ import pytest
 from conftest import PKG, ROOT
 
 BIN = os.path.join(PKG, "mps_siever")
+FAULTS_BIN = os.path.join(PKG, "mps_siever_faults")
 INT64_MAX = 2**63 - 1
 INT64_MIN = -(2**63)
 
 
-@pytest.fixture(scope="session")
-def siever_bin():
+def _build(target):
     srcs = [os.path.join(PKG, "host", f) for f in os.listdir(os.path.join(PKG, "host"))]
     srcs.append(os.path.join(ROOT, "include", "mps_gpu.h"))
-    if not os.path.exists(BIN) or os.path.getmtime(BIN) < max(os.path.getmtime(f) for f in srcs):
-        subprocess.run(["make", "-s", "-C", PKG, "mps_siever"], check=True)
-    return BIN
+    path = os.path.join(PKG, target)
+    if not os.path.exists(path) or os.path.getmtime(path) < max(os.path.getmtime(f) for f in srcs):
+        subprocess.run(["make", "-s", "-C", PKG, target], check=True)
+    return path
+
+
+@pytest.fixture(scope="session")
+def siever_bin():
+    return _build("mps_siever")
+
+
+@pytest.fixture(scope="session")
+def faults_bin():
+    return _build("mps_siever_faults")
 
 
 # ---------------------------------------------------- test-only restatement --
@@ -199,6 +210,48 @@ def test_prime_ini_written(siever_bin, tmp_path):
     assert (tmp_path / "prime.ini").read_text() == ini
 
 
+def test_factor_numbers_in_hex_and_octal(siever_bin, tmp_path):
+    # the reference reads b..N1 with its 128-bit type's string reading: "0x" hex, leading-0 octal
+    got = json.loads(_run_entry_line(siever_bin, tmp_path, "Factor=0x2,-031,0100,0x3e8,00,012,2,1"))
+    assert (got["b"], got["c"], got["P0"], got["P1"], got["N0"], got["N1"]) == (2, -25, 64, 1000, 0, 10)
+    assert got["prp"] == [1, 3, 5, 7, 9]
+
+
+def _run_entry_line(bin_path, tmp_path, line, relations=()):
+    rel = tmp_path / "rel.p"
+    rel.write_text("".join(f"{p}, {M}, {q}\n" for p, M, q in relations))
+    out = subprocess.run([bin_path, "--results-entry", str(rel), line, "t"], capture_output=True, text=True,
+                         check=True)
+    return out.stdout.strip()
+
+
+def test_gpu_strict_without_device(siever_bin, tmp_path):
+    # no usable device (an index no machine has): GPU_strict stops with the reference's message
+    (tmp_path / "prime.ini").write_text("CPU_count=1\nMemoryAllowed=64\nUseGPU=1\nGPU_device=999\nGPU_strict=1\n")
+    (tmp_path / "worktodo.txt").write_text("Factor=2,-25,1000000,2000000,0,1000,2,1\n")
+    r = subprocess.run([siever_bin], cwd=tmp_path, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 1
+    assert "[FATAL] GPU_strict=1 but no usable GPU backend; not sieving on the CPU" in r.stderr
+    assert not (tmp_path / "results.json").exists()
+
+
+def test_bad_prime_ini_value(siever_bin, tmp_path):
+    # std::stoi's error escapes to main, as in the reference (Siever.cpp:209-211)
+    (tmp_path / "prime.ini").write_text("CPU_count=four\nMemoryAllowed=64\n")
+    r = subprocess.run([siever_bin], cwd=tmp_path, capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1
+    assert "[FATAL] Unhandled exception: stoi" in r.stderr
+
+
+def test_malformed_relation_line(siever_bin, tmp_path):
+    rel = tmp_path / "rel.p"
+    rel.write_text("1000003, 5, 7\nnot a relation\n")
+    r = subprocess.run([siever_bin, "--results-entry", str(rel), "Factor=2,-25,10,100,0,10", "t"],
+                       capture_output=True, text=True)
+    assert r.returncode == 1
+    assert "Malformed relation line: not a relation" in r.stderr
+
+
 # ---------------------------------------------------------------- GPU tests --
 
 def _golden_case(golden, predicate):
@@ -284,3 +337,80 @@ def test_resume_reference_checkpoint(siever_bin, tmp_path, oracle):
     assert r.returncode == 0, r.stderr[-2000:]
     assert f"Checkpoint recovered: new P0 = {want[9][0]}" in r.stderr
     assert sorted(_parse_relations((tmp_path / "relations.p").read_text())) == want
+
+
+def _entries_without_time(path):
+    data = json.loads(path.read_text())
+    for e in data:
+        e.pop("Timestamp")
+    return data
+
+
+def _reference_run(siever_bin, tmp_path, items, memory_mb):
+    ref = tmp_path / "uninterrupted"
+    ref.mkdir()
+    _write_job(ref, items, memory_mb=memory_mb)
+    r = subprocess.run([siever_bin], cwd=ref, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    return (ref / "relations.p").read_text(), _entries_without_time(ref / "results.json")
+
+
+# two items, 2^24-integer chunks (MemoryAllowed=16 MB, CPU_count=1): 6 + 3 chunks
+STOP_ITEMS = [(2, -25, 10**9, 10**9 + 10**8, 0, 100_000, 2, 1),
+              (10, 111, 10**9, 10**9 + 5 * 10**7, 0, 10**7, 6, 4)]
+
+
+@pytest.mark.gpu
+def test_gpu_strict_declined_chunk_then_resume(siever_bin, faults_bin, tmp_path):
+    """GPU_strict=1 and a chunk the device declines (injected on the host):
+    the run stops as the reference's does (the INFO line naming the chunk,
+    then FATAL "Worker pool failed", exit 1) with the finished chunks kept;
+    the next run resumes and ends with the uninterrupted run's files."""
+    want_rel, want_results = _reference_run(siever_bin, tmp_path, STOP_ITEMS, 16)
+    run = tmp_path / "strict"
+    run.mkdir()
+    _write_job(run, STOP_ITEMS, memory_mb=16)
+    with open(run / "prime.ini", "a") as f:
+        f.write("GPU_strict=1\n")
+    env = dict(os.environ, MPS_SIEVER_DECLINE_CHUNK="3")
+    r = subprocess.run([faults_bin], cwd=run, capture_output=True, text=True, timeout=600, env=env)
+    assert r.returncode == 1
+    lo = 10**9 + 3 * (1 << 24)
+    assert (f"[INFO] GPU_strict=1: the GPU sieve declined the chunk starting at {lo}; "
+            "stopping instead of sieving on the CPU") in r.stderr
+    assert r.stderr.rstrip().endswith("[FATAL] Worker pool failed")
+    assert (run / "core_progress.txt").read_text().split()[-1] == str(lo)
+    assert not (run / "results.json").exists()
+    r = subprocess.run([siever_bin], cwd=run, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert f"Checkpoint recovered: new P0 = {lo}" in r.stderr
+    assert (run / "relations.p").read_text() == want_rel
+    assert _entries_without_time(run / "results.json") == want_results
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("after", [0, 4, 7])
+def test_sigint_between_chunks_then_resume(siever_bin, faults_bin, tmp_path, after):
+    """SIGINT delivered between chunks (raised by the program itself after
+    chunk `after`, through its real handler): the run ends with the
+    checkpoint kept; the next run resumes to the uninterrupted run's
+    relations.p and results.json.  A stop inside the second item (chunk 7)
+    is resumed as with the reference: the finished first line is removed
+    from worktodo.txt before the restart (every run redoes all listed items)."""
+    want_rel, want_results = _reference_run(siever_bin, tmp_path, STOP_ITEMS, 16)
+    run = tmp_path / "stopped"
+    run.mkdir()
+    _write_job(run, STOP_ITEMS, memory_mb=16)
+    env = dict(os.environ, MPS_SIEVER_SIGNAL_AFTER=str(after))
+    r = subprocess.run([faults_bin], cwd=run, capture_output=True, text=True, timeout=600, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "Shutdown: checkpoint preserved in core_*.p files" in r.stderr
+    first_done = after >= 6                               # item 1 is chunks 0-5
+    assert (run / "results.json").exists() == first_done
+    if first_done:
+        (run / "worktodo.txt").write_text(_factor_line(STOP_ITEMS[1]) + "\n")
+    r = subprocess.run([siever_bin], cwd=run, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "Checkpoint recovered: new P0 = " in r.stderr
+    assert (run / "relations.p").read_text() == want_rel
+    assert _entries_without_time(run / "results.json") == want_results

@@ -26,7 +26,13 @@ def _free_port() -> int:
         return s.getsockname()[1]
 
 
-def _rank_main(rank: int, world: int, port: int, out_dir: str, bin_path: str):
+def _oracle_slice(lo, hi, spec):
+    from oracle.oracle import Oracle, make_item
+    b, c, _, _, N0, N1, mod, res = spec
+    return Oracle().relations(lo, hi, make_item(b, c, lo, hi, N0, N1, mod, res), threads=2)
+
+
+def _rank_main(rank: int, world: int, port: int, out_dir: str, bin_path: str, spec=SPEC):
     import datetime
     import sys
     for p in (ROOT, PKG):
@@ -38,12 +44,10 @@ def _rank_main(rank: int, world: int, port: int, out_dir: str, bin_path: str):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
     try:
-        b, c, P0, P1, N0, N1, mod, res = SPEC
-        lo, hi = multi_gpu.shard_bounds(P0, P1, world, rank)
-        rels = Oracle().relations(lo, hi, make_item(b, c, lo, hi, N0, N1, mod, res), threads=2)
+        rels = multi_gpu.slice_relations(_oracle_slice, spec, world, rank)
         merged = multi_gpu.gather_relations(dist, rels, rank, world)
         if rank == 0:
-            multi_gpu.write_outputs(out_dir, SPEC, merged, siever_bin=bin_path)
+            multi_gpu.write_outputs(out_dir, spec, merged, siever_bin=bin_path)
         else:
             assert merged is None
         dist.barrier()
@@ -95,6 +99,26 @@ def test_two_rank_gloo(siever_bin, tmp_path, oracle):  # noqa: F811
     assert got == want
     entry = json.loads((tmp_path / "results.json").read_text())[0]
     assert entry == _entry(SPEC, want, entry["Timestamp"])
+
+
+def test_two_rank_gloo_range_narrower_than_world(siever_bin, tmp_path, oracle):  # noqa: F811
+    """A P range of one integer over two ranks: rank 0's slice is empty, it
+    computes nothing and still joins the gather; the result is the whole item's."""
+    from oracle.oracle import make_item
+    spec = (2, -25, 1_000_037, 1_000_038, 0, 20_000, 1, 0)      # one prime
+    world, port = 2, _free_port()
+    assert multi_gpu.shard_bounds(spec[2], spec[3], world, 0) == (spec[2], spec[2])
+    ctx = mp.get_context("spawn")
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, str(tmp_path), siever_bin, spec))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=300)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    want = oracle.relations(spec[2], spec[3], make_item(*spec))
+    entry = json.loads((tmp_path / "results.json").read_text())[0]
+    assert entry == _entry(spec, want, entry["Timestamp"])
 
 
 def test_merge_results_of_slices(oracle):
