@@ -66,14 +66,18 @@ typedef struct mps_tuning {
     uint32_t max_baby;          /* cap on the baby-step count (0: what the table holds)        */
     uint32_t bsgs_warps;        /* warps per BSGS block (0: 4)                                 */
     uint32_t class_modulus;     /* Q of the power-residue split g = gcd(Q, p-1)
-                                   (0: lcm(mod, 5040), or 5040 when that exceeds 100800)       */
+                                   (0: lcm(mod, 5040), or 5040 when that exceeds 100800;
+                                    1: lcm(mod, 2), the reference's plain-method filter)       */
     uint32_t full_mr;           /* 1: 12-base Miller-Rabin on every filter survivor (eager)    */
     uint32_t plain;             /* 1: plain per-chunk path (host sync between stages)          */
     uint32_t chains;            /* BSGS chains per lane, 1, 2 or 4 (0: 2)                      */
     uint32_t graphs_off;        /* 1: launch waves directly instead of replaying CUDA graphs   */
     uint32_t table_kind;        /* BSGS table: 0 = four 16-bit fingerprints per 64-bit word,
-                                   1 = one 32-bit key per slot                                 */
-    uint32_t reserved[4];
+                                   1 = one 32-bit key per slot, 2 = one 16-bit fingerprint
+                                   per slot, read with one 16-bit load per probe               */
+    uint32_t load_shift;        /* table kind 2: a prime's table is at least 2^load_shift times
+                                   its baby-step count (0: 2)                                  */
+    uint32_t reserved[3];
 } mps_tuning;
 
 /* Counters of the last call (all chunks of it). */
@@ -88,6 +92,9 @@ typedef struct mps_stats {
     uint64_t bsgs_launches;
     uint64_t kernel_launches;   /* kernels of this library launched             */
     uint64_t bsgs_steps;        /* baby + giant steps (Montgomery multiplies) done by the BSGS */
+    double   sieve_ms;          /* device time of the sieve kernel (CUDA events)  */
+    double   prep_ms;           /* device time of the prep kernel                 */
+    double   order_ms;          /* device time of the order kernel                */
 } mps_stats;
 
 /* ---- context (replaces CudaSiever::init, Cuda.hpp:198-257) ---- */
@@ -134,13 +141,21 @@ int mps_batch_relations(mps_ctx* ctx, const mps_item* items, size_t n_items, mps
 int mps_take_relations(mps_ctx* ctx, mps_relation* out, uint32_t* out_item, size_t cap, size_t* n_out);
 
 /* ---- serving: continuous batching of Factor= items (no counterpart in the reference) ----
- * A server owns a device context and a worker thread.  Submitted items wait
- * until admitted (fewer than max_active in flight and their pieces' device
- * memory within mem_budget_bytes); every wave takes one piece of
- * piece_odds odd numbers from each in-flight item in turn, so items that
- * arrive while others run join the next wave.  Per-item progress is kept
- * in a device table (mps_serve_checkpoint).  Results equal
- * mps_item_relations on the same item. */
+ * A server owns a device context, a worker thread and a device pool of
+ * min(mem_budget_bytes, 90% of the free device memory), allocated by
+ * mps_serve_open.  Every admitted item holds a reservation in that pool: a
+ * device buffer for its relations, sized at twice its expected relation
+ * count plus 256, which the commit kernel fills wave by wave (the item's
+ * device-resident result; a result that outgrows it comes from the host copy
+ * of the wave results instead).  Submitted items wait, in arrival order,
+ * until fewer than max_active are in flight and their reservation fits in
+ * the pool; an item larger than the whole pool fails with MPS_E_CAPACITY.
+ * Every wave takes one piece of piece_odds odd numbers from each in-flight
+ * item in turn, so items that arrive while others run join the next wave;
+ * the sieve segments, BSGS entries and baby-step tables of a wave live in
+ * the server's two fixed wave buffers.  Per-item progress is kept in a
+ * device table (mps_serve_checkpoint).  Results equal mps_item_relations on
+ * the same item. */
 typedef struct mps_server mps_server;
 typedef struct mps_serve_config {
     uint32_t struct_size;       /* sizeof(mps_serve_config)                  */
@@ -157,6 +172,9 @@ typedef struct mps_serve_status {
     uint64_t relations;
     double   latency_ms;        /* submit -> done                             */
     double   queue_ms;          /* submit -> admitted                         */
+    uint64_t reserved_bytes;    /* the item's reservation in the device pool  */
+    int32_t  relations_on_device; /* 1: the result was read from its device buffer */
+    int32_t  pad;
 } mps_serve_status;
 int mps_serve_config_default(mps_serve_config* cfg);
 int mps_serve_open(int device, const mps_tuning* tuning, const mps_serve_config* cfg, mps_server** out);
@@ -165,9 +183,43 @@ int mps_serve_submit(mps_server* sv, const mps_item* item, uint64_t* ticket);
 int mps_serve_wait(mps_server* sv, uint64_t ticket, double timeout_s, mps_serve_status* status);
 int mps_serve_result(mps_server* sv, uint64_t ticket, mps_relation* out, size_t cap, size_t* n_out);
 int mps_serve_release(mps_server* sv, uint64_t ticket);
+/* The reservation pool: its size, the bytes reserved by admitted items, and
+ * the items in flight and waiting. */
+int mps_serve_pool(mps_server* sv, uint64_t* pool_bytes, uint64_t* reserved_bytes, uint32_t* active,
+                   uint32_t* queued);
 /* Device-resident progress of an item: every p below *p_done sieved, *n_rel relations. */
 int mps_serve_checkpoint(mps_server* sv, uint64_t ticket, uint64_t* p_done, uint64_t* n_rel);
 int mps_serve_close(mps_server* sv);
+
+/* ---- autotuner (no counterpart in the reference, which sizes its baby-step table per
+ * item, Cuda.hpp:342-348, and picks m and Gc per prime, Gpu.hpp:553-573) ----
+ * For every item class among items -- the bit length of K (the item's count of
+ * in-class exponents), the class modulus, the decimal digits of P0 -- times
+ * each candidate BSGS configuration (table kind, table load, chains per lane,
+ * warps per block) with CUDA events on a calibration slice of the item (its
+ * first 2^25 integers), checks that every candidate gives the same relations,
+ * and keeps the fastest for the class.  Later calls on items of a tuned class
+ * use it (per item; a batched wave uses the configuration of its item with
+ * the largest K).  One report per class tuned; MPS_E_CAPACITY if cap is too
+ * small (*n_out = the number of classes).  The tuning changes speed only:
+ * relations are identical under every configuration. */
+typedef struct mps_tune_report {
+    uint32_t k_bits;              /* class: bit length of K                              */
+    uint32_t mod;                 /* class: class modulus (capped at 4095)               */
+    uint32_t p_digits;            /* class: decimal digits of P0, minus one              */
+    uint32_t candidates;          /* configurations timed                                */
+    uint32_t table_kind, load_shift, chains, warps;   /* the configuration chosen        */
+    double   best_ns_per_prime;   /* BSGS time per prime reaching the BSGS, chosen       */
+    double   default_ns_per_prime;/* the same under the context's tuning fields          */
+    uint64_t calib_bsgs_primes;   /* primes of the calibration slice reaching the BSGS   */
+} mps_tune_report;
+int mps_autotune(mps_ctx* ctx, const mps_item* items, size_t n_items, mps_tune_report* out, size_t cap,
+                 size_t* n_out);
+/* The tuned classes as text ("mps-tune 1" then one line per class); mps_open
+ * loads the file named by the environment variable MPS_TUNE_CACHE, if set. */
+int mps_tune_save(const mps_ctx* ctx, const char* path);
+int mps_tune_load(mps_ctx* ctx, const char* path);
+int mps_tune_clear(mps_ctx* ctx);
 
 /* Number of primes in [lo, hi) counted on the device (the unit of the
  * sieved-primes/s metric; not part of the relation path). */
@@ -179,17 +231,23 @@ int mps_count_primes(mps_ctx* ctx, uint64_t lo, uint64_t hi, uint64_t* count);
  * 2^49), and 32-bit integer multiply-adds per second (the integer pipe). */
 int mps_measure_peaks(mps_ctx* ctx, double* fmul_per_s, double* mmul_per_s, double* imad_per_s);
 
+/* Shared-memory ceiling of the segment sieve, measured on this device:
+ * conflict-free 32-bit shared-memory atomicOr operations per second. */
+int mps_measure_smem_peak(mps_ctx* ctx, double* atomic_or_per_s);
+
 /* ---- relations of one small range without allocating (no counterpart in the reference) ----
  * For callers that cannot allocate device memory where they sieve: their
  * device memory belongs to another framework's pool allocator, or cudaMalloc
  * / cudaFree (which synchronise the device) are not allowed in their loop.
- * Same result as mps_chunk_relations with the default tuning, on the calling
- * thread's current device and the default stream, with no context.  All
- * scratch is one static device array of 8 MiB that every GPU loading this
- * library holds until exit; its address is looked up on the first call on
- * each device (make that first call before any stream capture).  Calls share
- * that array, so calls that overlap on the GPU race and must not be made.
- * hi - lo must not exceed 2^19 (MPS_E_RANGE otherwise); hi <= 2^62. */
+ * Same relations as mps_chunk_relations with the default tuning, on the
+ * calling thread's current device and its per-thread default stream
+ * (cudaStreamPerThread), with no context.  All scratch is one static device
+ * array of 8 MiB that every GPU loading this library holds until exit; its
+ * address is looked up on the first call on each device (make that first
+ * call before any stream capture).  Calls on one device share its array, so
+ * two calls that overlap on the same GPU race and must not be made; calls on
+ * different devices may overlap.  hi - lo must not exceed 2^19 (MPS_E_RANGE
+ * otherwise); hi <= 2^62. */
 int mps_chunk_relations_noalloc(uint64_t lo, uint64_t hi, const mps_item* item,
                                 mps_relation* out, size_t cap, size_t* n_out);
 

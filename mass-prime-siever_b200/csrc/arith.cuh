@@ -94,48 +94,49 @@ __device__ __forceinline__ u32 gcd32(u32 a, u32 b) {
     return a;
 }
 
-// Jacobi symbol (a/n) for odd n (binary algorithm, Gpu.hpp:213-226); strips
-// all factors of two of a at once.
-__device__ __forceinline__ int jacobi(u64 a, u64 n) {
+// Jacobi symbol (a/n) for odd n < 2^32, a < n: the binary algorithm (strip
+// twos with (2/n) = -1 iff n == 3, 5 mod 8; swap with reciprocity, sign -1
+// iff both are 3 mod 4).  Returns 1, -1, or 0 when gcd(a, n) > 1.
+__device__ __forceinline__ int jacobi32(u32 a, u32 n) {
     u32 neg = 0;
     while (a != 0) {
-        const int tz = __ffsll((long long)a) - 1;
+        const int tz = __ffs((int)a) - 1;
         a >>= tz;
-        const u32 n8 = (u32)n & 7u;
-        if ((tz & 1) && (n8 == 3u || n8 == 5u)) neg ^= 1u;
+        if ((tz & 1) && ((n & 7u) == 3u || (n & 7u) == 5u)) neg ^= 1u;
         if (a < n) {
-            const u64 x = a;
+            const u32 x = a;
             a = n;
             n = x;
-            if ((a & n & 3ull) == 3ull) neg ^= 1u;
+            if ((a & n & 3u) == 3u) neg ^= 1u;
         }
         a -= n;
     }
     return n == 1 ? (neg ? -1 : 1) : 0;
 }
 
-// Strong probable-prime test of p (odd, > 2) to base 2, in the Montgomery
-// form of `M`: 2^d by square-and-double.
-__device__ __forceinline__ bool sprp2(const Mont& M) {
-    const u64 p = M.p;
-    const u64 pm1 = p - 1;
-    const int s = __ffsll((long long)pm1) - 1;
-    const u64 d = pm1 >> s;
-    const u64 minus_one = p - M.one;
-    int k = 63 - __clzll((long long)d);
-    u64 x = M.dbl(M.one);          // 2^1 (top bit of d)
-    for (--k; k >= 0; --k) {
-        x = M.mul(x, x);
-        if ((d >> k) & 1) x = M.dbl(x);
+// x mod o for an odd o < 2^32 from rcp = floor((2^64 - 1) / o).
+__device__ __forceinline__ u32 mod_small(u64 x, u32 o, u64 rcp) {
+    const u64 q = __umul64hi(x, rcp);
+    u64 r = x - q * o;
+    if (r >= o) r -= o;
+    return (u32)r;
+}
+
+// The Jacobi symbol (x/p) for odd p > o and x = (-1)^neg 2^k o, o odd:
+// (-1/p) = -1 iff p == 3 mod 4, (2/p) = -1 iff p == 3, 5 mod 8, and by
+// reciprocity (o/p) = (p mod o / o), negated iff o and p are both 3 mod 4.
+// 0 when gcd(o, p) > 1.
+__device__ __forceinline__ int jacobi_small(u64 p, u32 neg, u32 k, u32 o, u64 rcp) {
+    const u32 p8 = (u32)p & 7u;
+    u32 flip = 0;
+    if (neg && (p8 & 3u) == 3u) flip ^= 1u;
+    if ((k & 1u) && (p8 == 3u || p8 == 5u)) flip ^= 1u;
+    int j = 1;
+    if (o > 1) {
+        j = jacobi32(mod_small(p, o, rcp), o);
+        if ((o & 3u) == 3u && (p8 & 3u) == 3u) flip ^= 1u;
     }
-    x = M.norm(x);
-    if (x == M.one || x == minus_one) return true;
-    for (int r = 1; r < s; ++r) {
-        x = M.norm(M.mul(x, x));
-        if (x == minus_one) return true;
-        if (x == M.one) return false;
-    }
-    return false;
+    return flip ? -j : j;
 }
 
 // Strong test to base a (a < p), Montgomery form.

@@ -6,6 +6,7 @@
 // in the default (persistent) mode the four kernels are queued back to back
 // and the host waits once per chunk, for the relation count.
 #include "../../include/mps_gpu.h"
+#include "mps_item.cuh"
 #include "mps_kernels.cuh"
 
 #include <algorithm>
@@ -13,6 +14,7 @@
 #include <cmath>
 #include <condition_variable>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -27,7 +29,6 @@ using namespace mps;
 namespace {
 
 constexpr u64 kTwo62 = 1ull << 62;
-constexpr u64 kMaxNSpan = 10000000ull;   // N1 - N0 <= 10^7 (Config.hpp:187-190)
 
 // Odd primes 3..65521 and their division constants.
 struct HostTables {
@@ -54,21 +55,32 @@ const HostTables& host_tables() {
     return t;
 }
 
-u64 gcd_u64(u64 a, u64 b) {
-    while (b) {
-        const u64 t = a % b;
-        a = b;
-        b = t;
-    }
-    return a;
-}
-
 }  // namespace
+
+// One BSGS launch configuration (what the autotuner chooses per item class):
+// the table kind, its load (table kind 2), chains per lane and warps per block.
+struct BsgsCfg {
+    u32 kind = 0, load_shift = kDefaultLoadShift, chains = 2, warps = 4;
+    bool operator==(const BsgsCfg& o) const {
+        return kind == o.kind && load_shift == o.load_shift && chains == o.chains && warps == o.warps;
+    }
+    bool operator!=(const BsgsCfg& o) const { return !(*this == o); }
+};
+
+// A tuned configuration with the calibration that chose it.
+struct TuneEntry {
+    BsgsCfg cfg;
+    double ns_per_prime = 0;       // BSGS device time per prime of the calibration slice
+};
+
+// Events bracketing the four kernels of a chunk or wave: [2k] before and
+// [2k + 1] after stage k (0 sieve, 1 prep, 2 BSGS, 3 order).
+constexpr int kStageEvents = 8;
 
 // One of the two in-flight wave slots of the batched engine.
 struct WaveSlot {
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev_b0 = nullptr, ev_b1 = nullptr;
+    cudaEvent_t evk[kStageEvents] = {};   // around sieve, prep, BSGS, order
     u64* d_surv = nullptr;
     u32* d_surv_item = nullptr;
     u64 surv_cap = 0;
@@ -81,9 +93,14 @@ struct WaveSlot {
     Counters* h_ctr = nullptr;        // pinned
     WaveDesc* d_wave = nullptr;
     WaveDesc* h_wave = nullptr;       // pinned
-    cudaGraphExec_t graph = nullptr;
-    u32 graph_tbits = 0;
-    const DevItem* graph_items = nullptr;
+    // captured wave graphs of this slot, one per launch shape (tables, configuration) seen
+    struct Graph {
+        cudaGraphExec_t exec = nullptr;
+        u32 tbits = 0;
+        BsgsCfg cfg;
+    };
+    std::vector<Graph> graphs;
+    const DevItem* graph_items = nullptr;     // the buffers the graphs were captured with
     const ItemState* graph_state = nullptr;
     bool busy = false;
     std::vector<std::pair<u64, u64>> ranges;   // (lo, hi) of each run in flight
@@ -96,6 +113,7 @@ struct mps_ctx {
     size_t smem_optin = 227 * 1024;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evb0 = nullptr, evb1 = nullptr;
+    cudaEvent_t evk[kStageEvents] = {};
     mps_tuning tun{};
     std::string err;
     bool poisoned = false;
@@ -120,6 +138,8 @@ struct mps_ctx {
     WaveSlot slot[2];
     bool slots_ready = false;
     std::vector<u64> item_K;           // K of each item on the device (table sizing)
+    std::vector<BsgsCfg> item_cfg;     // BSGS configuration of each item on the device
+    std::map<u64, TuneEntry> tuned;    // autotuned configurations by item class (tune_key)
     std::vector<RawRelation> last;     // relations of the last call (kept for mps_take_relations)
 
     SieveTables tables() const { return SieveTables{d_sp, d_rcp, d_inv}; }
@@ -143,6 +163,18 @@ int cuda_fail(mps_ctx* c, cudaError_t e, const char* what) {
         cudaError_t e_ = (call);                         \
         if (e_ != cudaSuccess) return cuda_fail(c, e_, what); \
     } while (0)
+
+// Adds the device time of each stage of a finished chunk or wave to the stats.
+int add_stage_times(mps_ctx* c, cudaEvent_t const* ev) {
+    float ms[kStageEvents / 2] = {0, 0, 0, 0};
+    for (int k = 0; k < kStageEvents / 2; ++k) CK(cudaEventElapsedTime(&ms[k], ev[2 * k], ev[2 * k + 1]), "event time");
+    c->stats.sieve_ms += ms[0];
+    c->stats.prep_ms += ms[1];
+    c->stats.bsgs_ms += ms[2];
+    c->stats.order_ms += ms[3];
+    c->stats.bsgs_launches += 1;
+    return MPS_OK;
+}
 
 template <class T>
 int ensure(mps_ctx* c, T** ptr, u64* cap, u64 need, const char* what) {
@@ -168,85 +200,88 @@ int ensure_rel(mps_ctx* c, u64 need) {
     return MPS_OK;
 }
 
-// Baby-step table size for the item: 4 << tbits bytes per warp, at most
+u32 load_shift_of(const mps_ctx* c) { return c->tun.load_shift ? std::min<u32>(c->tun.load_shift, 4) : kDefaultLoadShift; }
+
+// The configuration the tuning fields ask for.
+BsgsCfg default_cfg(const mps_ctx* c) {
+    BsgsCfg g;
+    g.kind = c->tun.table_kind;
+    g.load_shift = load_shift_of(c);
+    g.chains = c->tun.chains ? c->tun.chains : 2;
+    g.warps = c->tun.bsgs_warps ? c->tun.bsgs_warps : 4;
+    return g;
+}
+
+// Item class of the autotuner: the bit length of K (the in-class exponent
+// count, which sets the baby/giant split), the class modulus (which sets the
+// power-residue split, capped at 4095) and the decimal digits of P0 (prime
+// density, and FP64 or integer arithmetic).
+u64 tune_key(u64 K, u64 cm, u64 P0) {
+    u64 kb = 0;
+    while ((K >> kb) != 0) ++kb;
+    u64 pd = 0;
+    for (u64 x = P0; x >= 10; x /= 10) ++pd;
+    return (kb << 40) | (std::min<u64>(cm, 4095) << 8) | pd;
+}
+
+// The configuration for an item: the tuned one of its class, else the default.
+BsgsCfg cfg_for(const mps_ctx* c, u64 K, u64 cm, u64 P0) {
+    auto it = c->tuned.find(tune_key(K, cm, P0));
+    return it != c->tuned.end() ? it->second.cfg : default_cfg(c);
+}
+
+// Keys a table of 4 << tb bytes holds under configuration g.
+u32 table_holds(const BsgsCfg& g, u32 tb) {
+    if (g.kind == 0) return 1u << (tb - 1);
+    if (g.kind == 2) return 1u << (tb + 1 - g.load_shift);
+    return std::max<u32>((1u << tb) / 5, 1);
+}
+
+// Baby-step table size for an item: 4 << tbits bytes per warp, at most
 // 8 KB by default (keeps ~24 warps resident per SM).  Every prime's j-range
 // is at most K, so m_opt = ceil(sqrt(K)) baby steps balance the giant steps;
 // a wider N range than the table holds trades baby steps for giant steps.
 // Fingerprint table (table_kind 0): 2^(tbits-1) words of four keys, filled
 // to at most one key per word on average.  32-bit slots (table_kind 1):
-// 2^tbits slots, load at most 1/5 (a probe then reads one slot).
-void table_for(const mps_ctx* c, u64 K, u32* tbits, u32* max_baby) {
+// 2^tbits slots, load at most 1/5 (a probe then reads one slot).  16-bit
+// slots (table_kind 2): 2^(tbits+1) slots, a prime's keys at most
+// 2^-load_shift of them (up to 12 bits, 16 KB per warp, when load_shift > 2).
+void table_for(const mps_ctx* c, const BsgsCfg& g, u64 K, u32* tbits, u32* max_baby) {
     const u64 m_opt = (u64)std::ceil(std::sqrt((double)std::max<u64>(K, 1)));
-    const bool quad = c->tun.table_kind == 0;
-    const auto holds = [&](u32 tb) { return quad ? (1u << (tb - 1)) : std::max<u32>((1u << tb) / 5, 1); };
+    const u32 top = g.kind == 2 && g.load_shift > 2 ? 12 : 11;
     u32 tb = c->tun.table_bits;
     if (tb == 0) {
         tb = 6;
-        while (holds(tb) < m_opt && tb < 11) ++tb;
+        while (table_holds(g, tb) < m_opt && tb < top) ++tb;
     }
     tb = std::min<u32>(std::max<u32>(tb, 6), 14);
-    u32 mb = c->tun.max_baby ? c->tun.max_baby : holds(tb);
-    const u32 cap = quad ? (1u << tb) : (1u << tb) - 1;       // fingerprints: at most two keys per word
+    u32 mb = c->tun.max_baby ? c->tun.max_baby : table_holds(g, tb);
+    // room for the keys: fingerprint words hold four, 32-bit slots one, 16-bit slots one with load <= 1/2
+    const u32 cap = g.kind == 0 ? (1u << tb) : g.kind == 2 ? (1u << tb) : (1u << tb) - 1;
     mb = std::min<u32>(std::min<u32>(mb, kMaxBaby), cap);
     *tbits = tb;
     *max_baby = std::max<u32>(mb, 1);
 }
 
-// Validates an item the way load_worktodo does (Config.hpp:156-190) plus the
-// GPU path's range (P1 <= 2^62); fills the device-side constants.
-int make_dev_item(mps_ctx* c, const mps_item* it, u32 index, DevItem* d) {
-    if (!it) return fail(c, MPS_E_ARG, "item is NULL");
-    if (it->P0 >= it->P1) return fail(c, MPS_E_ARG, "requires P0 < P1");
-    if (it->P1 > kTwo62) return fail(c, MPS_E_RANGE, "P1 must not exceed 2^62");
-    if (it->N0 >= it->N1) return fail(c, MPS_E_ARG, "requires N0 < N1");
-    if ((unsigned __int128)((__int128)it->N1 - it->N0) > kMaxNSpan) return fail(c, MPS_E_RANGE, "range N1-N0 exceeds 10 million");
-    const u64 cm = it->mod == 0 ? 1 : it->mod;
-    if (it->res >= cm) return fail(c, MPS_E_ARG, "class must satisfy 0 <= res < mod");
-    std::memset(d, 0, sizeof(*d));
-    const __int128 b = (__int128)(((unsigned __int128)(u64)it->b_hi << 64) | it->b_lo);
-    const __int128 cc = (__int128)(((unsigned __int128)(u64)it->c_hi << 64) | it->c_lo);
-    const unsigned __int128 babs = b < 0 ? (unsigned __int128)0 - (unsigned __int128)b : (unsigned __int128)b;
-    const unsigned __int128 cabs = cc < 0 ? (unsigned __int128)0 - (unsigned __int128)cc : (unsigned __int128)cc;
-    d->babs_hi = (u64)(babs >> 64);
-    d->babs_lo = (u64)babs;
-    d->cabs_hi = (u64)(cabs >> 64);
-    d->cabs_lo = (u64)cabs;
-    d->b_neg = b < 0;
-    d->c_neg = cc < 0;
-    d->N0_raw = it->N0;
-    d->N1_raw = it->N1;
-    d->N0 = it->N0 < 0 ? 0 : (u64)it->N0;
-    d->N1 = it->N1 < 0 ? 0 : (u64)it->N1;
-    d->cm = cm;
-    d->n_start = d->N0 + ((it->res % cm) + cm - (d->N0 % cm)) % cm;
-    d->has_work = (it->N1 > 0 && d->n_start < d->N1) ? 1 : 0;
-    d->K = d->has_work ? (d->N1 - d->n_start + cm - 1) / cm : 0;
-    u64 Q = c->tun.class_modulus;
-    if (Q == 0) {
-        // the split modulus: 5040 = 2^4 3^2 5 7 (and the class modulus, when small)
-        const u64 l = cm / gcd_u64(cm, 5040) * 5040;
-        Q = l <= 100800 ? l : 5040;
-    }
-    if (Q < 2 || Q > (1u << 20) || (Q & 1)) return fail(c, MPS_E_ARG, "class_modulus must be even and <= 2^20");
-    // (at most 7 distinct prime factors below 2^20: 2*3*5*7*11*13*17 = 510510)
-    d->Q = (u32)Q;
-    d->Q_rcp = ~0ull / Q;
-    {
-        u64 x = Q;
-        d->qf_n = 0;
-        for (u64 l = 2; l * l <= x; ++l) {
-            if (x % l) continue;
-            d->qf_l[d->qf_n++] = (u32)l;
-            while (x % l == 0) x /= l;
-        }
-        if (x > 1) d->qf_l[d->qf_n++] = (u32)x;
-    }
-    d->cmQ = (u32)(cm % Q);
-    d->nsQ = (u32)(d->n_start % Q);
-    d->item_index = index;
+// The baby-step cap of a launch with configuration g and tables of 4 << tbits
+// bytes: no prime of the launch gets more, whatever its item's own sizing.
+u32 launch_m_cap(const mps_ctx* c, const BsgsCfg& g, u32 tbits) {
+    const u32 cap = g.kind == 0 ? (1u << tbits) : g.kind == 2 ? (1u << tbits) : (1u << tbits) - 1;
+    const u32 holds = c->tun.max_baby ? std::max(c->tun.max_baby, table_holds(g, tbits)) : table_holds(g, tbits);
+    return std::max<u32>(1, std::min<u32>(std::min<u32>(holds, cap), kMaxBaby));
+}
+
+// The device constants of an item (mps_item.cuh), with this context's split
+// modulus, the item's BSGS configuration (tuned or default) and its
+// baby-step sizing.
+int make_dev_item(mps_ctx* c, const mps_item* it, u32 index, DevItem* d, BsgsCfg* cfg = nullptr) {
+    const char* why = "";
+    if (int r = item_constants(it, c->tun.class_modulus, index, d, &why)) return fail(c, r, why);
+    const BsgsCfg g = cfg_for(c, d->K, d->cm, it->P0);
     u32 tb = 0, mb = 0;
-    table_for(c, d->K, &tb, &mb);
+    table_for(c, g, d->K, &tb, &mb);
     d->max_baby = mb;
+    if (cfg) *cfg = g;
     return MPS_OK;
 }
 
@@ -292,7 +327,7 @@ int bsgs_grid(mps_ctx* c, u32 tbits, u32 warps, int* grid) {
 
 // Relations of the primes of one device chunk [lo, hi) (at most chunk_odds
 // odd numbers) for item `item`, already on the device.  Appends RawRelations.
-int run_chunk(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, std::vector<RawRelation>& out) {
+int run_chunk(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, const BsgsCfg& g, std::vector<RawRelation>& out) {
     const u64 lo_odd = std::max<u64>(lo, 3) | 1ull;
     const u64 n_odds = lo_odd < hi ? (hi - lo_odd + 1) / 2 : 0;
     const u32 include_two = (lo <= 2 && hi > 2) ? 1 : 0;
@@ -304,9 +339,9 @@ int run_chunk(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, std::vector<RawRelati
     if (int r = ensure_rel(c, std::max<u64>(c->rel_cap, 1 << 18))) return r;
 
     u32 tbits, max_baby;
-    table_for(c, K, &tbits, &max_baby);
+    table_for(c, g, K, &tbits, &max_baby);
     (void)max_baby;
-    const u32 warps = c->tun.bsgs_warps ? c->tun.bsgs_warps : 4;
+    const u32 warps = g.warps;
 
     SieveArgs sa{};
     sa.lo_odd = lo_odd;
@@ -327,6 +362,7 @@ int run_chunk(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, std::vector<RawRelati
     pa.rel = c->d_rel;
     pa.rel_cap = c->rel_cap;
     pa.full_mr = c->tun.full_mr;
+    pa.m_cap = launch_m_cap(c, g, tbits);
 
     BsgsArgs ba{};
     ba.ent = c->d_ent;
@@ -335,8 +371,9 @@ int run_chunk(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, std::vector<RawRelati
     ba.rel_cap = c->rel_cap;
     ba.tbits = tbits;
     ba.warps_per_block = warps;
-    ba.chains = c->tun.chains ? c->tun.chains : 2;
-    ba.table_kind = c->tun.table_kind;
+    ba.chains = g.chains;
+    ba.table_kind = g.kind;
+    ba.load_shift = g.load_shift;
     ba.max_p = hi;
 
     OrderArgs oa{};
@@ -347,7 +384,9 @@ int run_chunk(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, std::vector<RawRelati
 
     cudaStream_t s = c->stream;
     CK(cudaMemsetAsync(c->d_ctr, 0, sizeof(Counters), s), "counter reset");
+    CK(cudaEventRecord(c->evk[0], s), "event");
     CK(launch_sieve(sa, c->tables(), c->d_surv, nullptr, c->surv_cap, c->d_ctr, s), "sieve launch");
+    CK(cudaEventRecord(c->evk[1], s), "event");
     int bgrid = 0;
     if (int r = bsgs_grid(c, tbits, warps, &bgrid)) return r;
     if (c->tun.plain) {
@@ -355,40 +394,43 @@ int run_chunk(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, std::vector<RawRelati
         CK(cudaMemcpyAsync(c->h_ctr, c->d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, s), "count read");
         CK(cudaStreamSynchronize(s), "sieve");
         const u64 ns = std::min<u64>(c->h_ctr->survivors, c->surv_cap);
+        CK(cudaEventRecord(c->evk[2], s), "event");
         CK(launch_prep(pa, c->d_ctr, (int)std::max<u64>((ns + 255) / 256, 1), s), "prep launch");
+        CK(cudaEventRecord(c->evk[3], s), "event");
         CK(cudaMemcpyAsync(c->h_ctr, c->d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, s), "count read");
         CK(cudaStreamSynchronize(s), "prep");
         const u64 ne = std::min<u64>(c->h_ctr->entries, c->ent_cap);
         ba.persistent = 0;
-        CK(cudaEventRecord(c->evb0, s), "event");
+        CK(cudaEventRecord(c->evk[4], s), "event");
         if (ne) CK(launch_bsgs(ba, c->d_ctr, (int)((ne + warps - 1) / warps), s), "bsgs launch");
-        CK(cudaEventRecord(c->evb1, s), "event");
+        CK(cudaEventRecord(c->evk[5], s), "event");
     } else {
+        CK(cudaEventRecord(c->evk[2], s), "event");
         CK(launch_prep(pa, c->d_ctr, grid_for(c, 16), s), "prep launch");
+        CK(cudaEventRecord(c->evk[3], s), "event");
         ba.persistent = 1;
-        CK(cudaEventRecord(c->evb0, s), "event");
+        CK(cudaEventRecord(c->evk[4], s), "event");
         CK(launch_bsgs(ba, c->d_ctr, bgrid, s), "bsgs launch");
-        CK(cudaEventRecord(c->evb1, s), "event");
+        CK(cudaEventRecord(c->evk[5], s), "event");
     }
+    CK(cudaEventRecord(c->evk[6], s), "event");
     CK(launch_order(oa, c->d_ctr, grid_for(c, 4), s), "order launch");
+    CK(cudaEventRecord(c->evk[7], s), "event");
     CK(cudaMemcpyAsync(c->h_ctr, c->d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, s), "count read");
     CK(cudaStreamSynchronize(s), "chunk");
-    float bms = 0;
-    CK(cudaEventElapsedTime(&bms, c->evb0, c->evb1), "event time");
-    c->stats.bsgs_ms += bms;
-    c->stats.bsgs_launches += 1;
+    if (int r = add_stage_times(c, c->evk)) return r;
     c->stats.kernel_launches += 4;
     const Counters h = *c->h_ctr;
     if (h.status & (kStatusSurvivorOverflow | kStatusEntryOverflow)) {
         // a denser range than the buffers were sized for: halve the chunk
         if (n_odds <= 1024) return fail(c, MPS_E_CUDA, "device buffers overflow on a tiny chunk");
         const u64 mid = lo_odd + 2 * (n_odds / 2);
-        if (int r = run_chunk(c, lo, mid, item, K, out)) return r;
-        return run_chunk(c, mid, hi, item, K, out);
+        if (int r = run_chunk(c, lo, mid, item, K, g, out)) return r;
+        return run_chunk(c, mid, hi, item, K, g, out);
     }
     if (h.status & kStatusRelationOverflow) {
         if (int r = ensure_rel(c, std::max<u64>(2 * c->rel_cap, h.relations + 1024))) return r;
-        return run_chunk(c, lo, hi, item, K, out);
+        return run_chunk(c, lo, hi, item, K, g, out);
     }
     if (h.status & kStatusOrderFailed) return fail(c, MPS_E_CUDA, "order computation did not factor p - 1");
     const u64 nr = h.relations;
@@ -421,12 +463,17 @@ int run_chunk(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, std::vector<RawRelati
 
 constexpr u64 kGraphRelations = 4096;    // relations copied back inside the graph
 
+void drop_graphs(WaveSlot& w) {
+    for (WaveSlot::Graph& g : w.graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    w.graphs.clear();
+}
+
 int slot_alloc(mps_ctx* c, WaveSlot& w) {
     const u64 chunk = c->tun.chunk_odds;
     if (!w.stream) {
         CK(cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking), "stream");
-        CK(cudaEventCreate(&w.ev_b0), "event");
-        CK(cudaEventCreate(&w.ev_b1), "event");
+        for (cudaEvent_t& ev : w.evk) CK(cudaEventCreate(&ev), "event");
         CK(cudaMalloc((void**)&w.d_ctr, sizeof(Counters)), "counters");
         CK(cudaMallocHost((void**)&w.h_ctr, sizeof(Counters)), "counters");
         CK(cudaMalloc((void**)&w.d_wave, sizeof(WaveDesc)), "wave descriptor");
@@ -438,15 +485,13 @@ int slot_alloc(mps_ctx* c, WaveSlot& w) {
         w.surv_cap = chunk + kMaxRuns + 16;
         CK(cudaMalloc((void**)&w.d_surv, w.surv_cap * sizeof(u64)), "survivor buffer");
         CK(cudaMalloc((void**)&w.d_surv_item, w.surv_cap * sizeof(u32)), "survivor items");
-        if (w.graph) cudaGraphExecDestroy(w.graph);
-        w.graph = nullptr;
+        drop_graphs(w);
     }
     if (w.ent_cap < std::max<u64>(chunk / 4, 1 << 16)) {
         if (w.d_ent) CK(cudaFree(w.d_ent), "cudaFree");
         w.ent_cap = std::max<u64>(chunk / 4, 1 << 16);
         CK(cudaMalloc((void**)&w.d_ent, w.ent_cap * sizeof(Entry)), "entry buffer");
-        if (w.graph) cudaGraphExecDestroy(w.graph);
-        w.graph = nullptr;
+        drop_graphs(w);
     }
     if (w.rel_cap < (1u << 16)) {
         w.rel_cap = 1u << 16;
@@ -458,30 +503,31 @@ int slot_alloc(mps_ctx* c, WaveSlot& w) {
 
 void slot_free(WaveSlot& w) {
     if (w.stream) cudaStreamSynchronize(w.stream);
-    if (w.graph) cudaGraphExecDestroy(w.graph);
+    drop_graphs(w);
     for (void* p : {(void*)w.d_surv, (void*)w.d_surv_item, (void*)w.d_ent, (void*)w.d_rel, (void*)w.d_ctr,
                     (void*)w.d_wave})
         if (p) cudaFree(p);
     for (void* p : {(void*)w.h_rel, (void*)w.h_ctr, (void*)w.h_wave})
         if (p) cudaFreeHost(p);
-    if (w.ev_b0) cudaEventDestroy(w.ev_b0);
-    if (w.ev_b1) cudaEventDestroy(w.ev_b1);
+    for (cudaEvent_t ev : w.evk)
+        if (ev) cudaEventDestroy(ev);
     if (w.stream) cudaStreamDestroy(w.stream);
     w = WaveSlot();
 }
 
 // The per-wave launch sequence on the slot's stream (captured or direct).
-int slot_enqueue(mps_ctx* c, WaveSlot& w, u32 tbits, bool capturing) {
+int slot_enqueue(mps_ctx* c, WaveSlot& w, u32 tbits, const BsgsCfg& g, bool capturing) {
     const cudaStream_t s = w.stream;
-    const u32 warps = c->tun.bsgs_warps;
+    const u32 warps = g.warps;
     PrepArgs pa{};
     pa.surv = w.d_surv; pa.surv_cap = w.surv_cap; pa.surv_item = w.d_surv_item; pa.item0 = 0;
     pa.items = c->d_items; pa.ent = w.d_ent; pa.ent_cap = w.ent_cap; pa.rel = w.d_rel; pa.rel_cap = w.rel_cap;
     pa.full_mr = c->tun.full_mr;
+    pa.m_cap = launch_m_cap(c, g, tbits);
     BsgsArgs ba{};
     ba.ent = w.d_ent; ba.ent_cap = w.ent_cap; ba.rel = w.d_rel; ba.rel_cap = w.rel_cap; ba.tbits = tbits;
-    ba.warps_per_block = warps; ba.persistent = 1; ba.chains = c->tun.chains ? c->tun.chains : 2;
-    ba.table_kind = c->tun.table_kind;
+    ba.warps_per_block = warps; ba.persistent = 1; ba.chains = g.chains;
+    ba.table_kind = g.kind; ba.load_shift = g.load_shift;
     ba.max_p = 0;   // per-entry arithmetic
     OrderArgs oa{};
     oa.rel = w.d_rel; oa.rel_cap = w.rel_cap; oa.items = c->d_items; oa.tables = c->tables();
@@ -489,15 +535,21 @@ int slot_enqueue(mps_ctx* c, WaveSlot& w, u32 tbits, bool capturing) {
     if (int r = bsgs_grid(c, tbits, warps, &bgrid)) return r;
     CK(cudaMemcpyAsync(w.d_wave, w.h_wave, sizeof(WaveDesc), cudaMemcpyHostToDevice, s), "wave upload");
     CK(cudaMemsetAsync(w.d_ctr, 0, sizeof(Counters), s), "counter reset");
-    CK(launch_sieve_wave(w.d_wave, c->tables(), w.d_surv, w.d_surv_item, w.surv_cap, w.d_ctr, grid_for(c, 8), s),
-       "sieve launch");
-    CK(launch_prep(pa, w.d_ctr, grid_for(c, 16), s), "prep launch");
     // external records: a captured graph records these events on every replay
     const unsigned ev_flags = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
-    CK(cudaEventRecordWithFlags(w.ev_b0, s, ev_flags), "event");
+    CK(cudaEventRecordWithFlags(w.evk[0], s, ev_flags), "event");
+    CK(launch_sieve_wave(w.d_wave, c->tables(), w.d_surv, w.d_surv_item, w.surv_cap, w.d_ctr, grid_for(c, 8), s),
+       "sieve launch");
+    CK(cudaEventRecordWithFlags(w.evk[1], s, ev_flags), "event");
+    CK(cudaEventRecordWithFlags(w.evk[2], s, ev_flags), "event");
+    CK(launch_prep(pa, w.d_ctr, grid_for(c, 16), s), "prep launch");
+    CK(cudaEventRecordWithFlags(w.evk[3], s, ev_flags), "event");
+    CK(cudaEventRecordWithFlags(w.evk[4], s, ev_flags), "event");
     CK(launch_bsgs(ba, w.d_ctr, bgrid, s), "bsgs launch");
-    CK(cudaEventRecordWithFlags(w.ev_b1, s, ev_flags), "event");
+    CK(cudaEventRecordWithFlags(w.evk[5], s, ev_flags), "event");
+    CK(cudaEventRecordWithFlags(w.evk[6], s, ev_flags), "event");
     CK(launch_order(oa, w.d_ctr, grid_for(c, 4), s), "order launch");
+    CK(cudaEventRecordWithFlags(w.evk[7], s, ev_flags), "event");
     CK(launch_commit(w.d_wave, w.d_rel, w.d_ctr, w.rel_cap, c->d_state, s), "commit launch");
     CK(cudaMemcpyAsync(w.h_ctr, w.d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, s), "count read");
     CK(cudaMemcpyAsync(w.h_rel, w.d_rel, kGraphRelations * sizeof(RawRelation), cudaMemcpyDeviceToHost, s),
@@ -505,30 +557,55 @@ int slot_enqueue(mps_ctx* c, WaveSlot& w, u32 tbits, bool capturing) {
     return MPS_OK;
 }
 
-int slot_launch(mps_ctx* c, WaveSlot& w, u32 tbits) {
-    if (c->tun.graphs_off) return slot_enqueue(c, w, tbits, false);
-    if (!w.graph || w.graph_tbits != tbits || w.graph_items != c->d_items || w.graph_state != c->d_state) {
-        if (w.graph) cudaGraphExecDestroy(w.graph);
-        w.graph = nullptr;
-        CK(bsgs_reserve_smem(bsgs_smem_bytes(tbits, c->tun.bsgs_warps)), "bsgs shared memory");
+int slot_launch(mps_ctx* c, WaveSlot& w, u32 tbits, const BsgsCfg& cfg) {
+    if (c->tun.graphs_off) return slot_enqueue(c, w, tbits, cfg, false);
+    if (w.graph_items != c->d_items || w.graph_state != c->d_state) {
+        drop_graphs(w);
+        w.graph_items = c->d_items;
+        w.graph_state = c->d_state;
+    }
+    cudaGraphExec_t exec = nullptr;
+    for (const WaveSlot::Graph& g : w.graphs)
+        if (g.tbits == tbits && g.cfg == cfg) exec = g.exec;
+    if (!exec) {
+        if (w.graphs.size() >= 8) drop_graphs(w);
+        CK(bsgs_reserve_smem(bsgs_smem_bytes(tbits, cfg.warps)), "bsgs shared memory");
         cudaGraph_t g = nullptr;
         CK(cudaStreamBeginCapture(w.stream, cudaStreamCaptureModeThreadLocal), "capture");
-        const int r = slot_enqueue(c, w, tbits, true);
+        const int r = slot_enqueue(c, w, tbits, cfg, true);
         cudaError_t e = cudaStreamEndCapture(w.stream, &g);
         if (r) {
             if (g) cudaGraphDestroy(g);
             return r;
         }
         if (e != cudaSuccess) return cuda_fail(c, e, "end capture");
-        e = cudaGraphInstantiate(&w.graph, g, 0);
+        e = cudaGraphInstantiate(&exec, g, 0);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) return cuda_fail(c, e, "graph instantiate");
-        w.graph_tbits = tbits;
-        w.graph_items = c->d_items;
-        w.graph_state = c->d_state;
+        WaveSlot::Graph entry;
+        entry.exec = exec;
+        entry.tbits = tbits;
+        entry.cfg = cfg;
+        w.graphs.push_back(entry);
     }
-    CK(cudaGraphLaunch(w.graph, w.stream), "graph launch");
+    CK(cudaGraphLaunch(exec, w.stream), "graph launch");
     return MPS_OK;
+}
+
+// The launch shape of a wave: the configuration of its item with the most
+// in-class exponents (whose BSGS dominates the wave), with tables large
+// enough for every item in it.
+void wave_shape(const mps_ctx* c, const WaveSlot& w, u32* tbits, BsgsCfg* g) {
+    u32 top = w.range_item[0];
+    for (u32 it : w.range_item)
+        if (c->item_K[it] > c->item_K[top]) top = it;
+    *g = c->item_cfg[top];
+    *tbits = 6;
+    for (u32 it : w.range_item) {
+        u32 tb, mb;
+        table_for(c, *g, c->item_K[it], &tb, &mb);
+        *tbits = std::max(*tbits, tb);
+    }
 }
 
 // Waits for the slot's wave and appends its relations; on a buffer overflow
@@ -538,20 +615,26 @@ int slot_finish(mps_ctx* c, WaveSlot& w, std::vector<RawRelation>& out) {
     w.busy = false;
     CK(cudaStreamSynchronize(w.stream), "wave");
     const Counters h = *w.h_ctr;
-    float bms = 0;
-    CK(cudaEventElapsedTime(&bms, w.ev_b0, w.ev_b1), "event time");
-    c->stats.bsgs_ms += bms;
-    c->stats.bsgs_launches += 1;
+    if (int r = add_stage_times(c, w.evk)) return r;
     c->stats.kernel_launches += 5;
     if (h.status & kStatusOrderFailed) return fail(c, MPS_E_CUDA, "order computation did not factor p - 1");
     if (h.status & (kStatusSurvivorOverflow | kStatusEntryOverflow | kStatusRelationOverflow)) {
+        // the commit kernel skipped this wave: redo its runs on the chunk path
+        // (which splits or grows as needed) and record each in the item table
         for (size_t i = 0; i < w.ranges.size(); ++i) {
             std::vector<RawRelation> part;
-            const DevItem* items = c->d_items;
-            (void)items;
-            if (int r = run_chunk(c, w.ranges[i].first, w.ranges[i].second, w.range_item[i],
-                                  c->item_K[w.range_item[i]], part))
+            const u32 item = w.range_item[i];
+            if (int r = run_chunk(c, w.ranges[i].first, w.ranges[i].second, item, c->item_K[item], c->item_cfg[item],
+                                  part))
                 return r;
+            // the chunk path is done with its relation buffer: stage the run's relations there
+            if (int r = ensure_rel(c, std::max<u64>(c->rel_cap, part.size()))) return r;
+            if (!part.empty())
+                CK(cudaMemcpyAsync(c->d_rel, part.data(), part.size() * sizeof(RawRelation), cudaMemcpyHostToDevice,
+                                   c->stream),
+                   "state update");
+            CK(launch_state_add(c->d_state, item, w.ranges[i].second, c->d_rel, part.size(), c->stream), "state update");
+            CK(cudaStreamSynchronize(c->stream), "state update");
             out.insert(out.end(), part.begin(), part.end());
         }
         return MPS_OK;
@@ -580,12 +663,6 @@ int run_waves(mps_ctx* c, const std::vector<u64>& lo, const std::vector<u64>& hi
     }
     for (WaveSlot& w : c->slot)
         if (int r = slot_alloc(c, w)) return r;
-    u32 tbits = 5;
-    for (size_t i = 0; i < lo.size(); ++i) {
-        u32 tb, mb;
-        table_for(c, c->item_K[i], &tb, &mb);
-        tbits = std::max(tbits, tb);
-    }
     const u64 chunk = c->tun.chunk_odds;
     int k = 0;
     WaveSlot* cur = nullptr;
@@ -597,7 +674,10 @@ int run_waves(mps_ctx* c, const std::vector<u64>& lo, const std::vector<u64>& hi
             cur->h_wave->runs[r].seg_begin = cur->h_wave->total_segs;
             cur->h_wave->total_segs += (cur->h_wave->runs[r].n_odds + kSieveSegOdds - 1) / kSieveSegOdds;
         }
-        if (int r = slot_launch(c, *cur, tbits)) return r;
+        u32 tbits;
+        BsgsCfg g;
+        wave_shape(c, *cur, &tbits, &g);
+        if (int r = slot_launch(c, *cur, tbits, g)) return r;
         cur->busy = true;
         k ^= 1;
         cur = nullptr;
@@ -665,15 +745,67 @@ struct ServeReq {
     u64 cursor = 0;                    // next P to hand to a wave
     u32 inflight = 0;                  // waves in flight with a piece of this item
     std::multiset<u64> piece_lo;       // low ends of this item's pieces in flight
-    u64 mem = 0;                       // device bytes reserved
+    u64 mem = 0;                       // device bytes its reservation takes (its relation buffer)
+    u64 pool_off = 0;                  // the reservation's offset in the server's pool, while admitted
+    bool relations_on_device = false;  // the result was read from the item's device buffer
     int state = 0;                     // 0 queued, 1 active, 2 done, 3 failed
     int error = 0;
     std::vector<RawRelation> rel;
     std::chrono::steady_clock::time_point t_submit, t_admit, t_done;
 };
 
+// First-fit allocator over a device pool [0, size), 256-byte granules; free
+// blocks kept by offset and merged with their neighbours on release.
+class PoolAlloc {
+public:
+    void reset(u64 size) {
+        free_.clear();
+        if (size) free_[0] = size;
+        total_ = size;
+        used_ = 0;
+    }
+    bool take(u64 bytes, u64* off) {
+        bytes = (bytes + 255) & ~255ull;
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second < bytes) continue;
+            *off = it->first;
+            const u64 rest = it->second - bytes, at = it->first + bytes;
+            free_.erase(it);
+            if (rest) free_[at] = rest;
+            used_ += bytes;
+            return true;
+        }
+        return false;
+    }
+    void give(u64 off, u64 bytes) {
+        bytes = (bytes + 255) & ~255ull;
+        used_ -= bytes;
+        auto it = free_.emplace(off, bytes).first;
+        auto next = std::next(it);
+        if (next != free_.end() && it->first + it->second == next->first) {
+            it->second += next->second;
+            free_.erase(next);
+        }
+        if (it != free_.begin()) {
+            auto prev = std::prev(it);
+            if (prev->first + prev->second == it->first) {
+                prev->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+    u64 used() const { return used_; }
+    u64 total() const { return total_; }
+
+private:
+    std::map<u64, u64> free_;
+    u64 total_ = 0, used_ = 0;
+};
+
 struct mps_server {
     mps_ctx* ctx = nullptr;
+    unsigned char* pool = nullptr;     // device memory the admitted items' reservations live in
+    PoolAlloc alloc;
     mps_serve_config cfg{};
     std::thread worker;
     std::mutex mu;
@@ -682,7 +814,6 @@ struct mps_server {
     std::map<u64, ServeReq> reqs;
     std::vector<u64> slot_owner;       // device item slot -> ticket (0: free)
     u64 next_ticket = 1;
-    u64 mem_used = 0;
     u32 active = 0;
     bool stop = false;
     int fatal = 0;
@@ -696,17 +827,34 @@ double ms_between(std::chrono::steady_clock::time_point a, std::chrono::steady_c
     return std::chrono::duration<double, std::milli>(b - a).count();
 }
 
-// Device bytes an item's pieces need: survivors (8 B) and entries (72 B) of
-// one piece (density of survivors ~ 2.2/ln(P0) of the odd numbers, at most
-// all of them below 10^6), and 4-byte table slots for the resident warps.
-u64 item_memory(const mps_server* sv, const DevItem& d, const mps_item& it) {
-    const double lp = std::log((double)std::max<u64>(it.P0, 16));
-    const double dens = std::min(1.0, 2.2 / lp + (it.P0 < 1000000 ? 0.3 : 0.0));
-    const u64 piece = std::min<u64>(sv->cfg.piece_odds, (it.P1 - it.P0) / 2 + 1);
-    u32 tb, mb;
-    table_for(sv->ctx, d.K, &tb, &mb);
-    const u64 tables = (u64)(4u << tb) * 64 * (u64)sv->ctx->num_sms;   // resident warps x slots x 4 B
-    return (u64)(piece * dens * (8.0 + 72.0 * 0.5)) + tables / 16 + sizeof(DevItem) + sizeof(ItemState);
+// The relations an item may give, for its device reservation: a prime p <= K
+// (K in-class exponents) can meet a whole period of b's order, so each of
+// those counts once; a larger p divides one of the K values with chance about
+// K/p, and the sum of K/p over the primes of [a, b) is about
+// K (ln ln b - ln ln a).  Twice that plus 256, at most 2^26.
+u64 expected_relations(const DevItem& d, const mps_item& it) {
+    const double K = (double)d.K;
+    const auto approx_pi = [](double x) { return x < 3 ? 0.0 : x / std::log(x); };
+    const double a = std::max<double>((double)it.P0, 2.0), b = (double)it.P1;
+    const double split = std::min(b, std::max(a, K + 1));
+    double e = split > a ? approx_pi(split) - approx_pi(a) : 0.0;
+    const double lo = std::max(split, 3.0);
+    if (b > lo) e += K * (std::log(std::log(b)) - std::log(std::log(lo)));
+    return (u64)std::min(2.0 * e + 256.0, (double)(1ull << 26));
+}
+
+// Reads a finished item's relations from its device buffer; false when they
+// did not all fit (the host copy of the wave results is used then).
+bool read_device_relations(mps_server* sv, const ServeReq& q, std::vector<RawRelation>* out) {
+    ItemState h{};
+    if (cudaMemcpy(&h, sv->ctx->d_state + q.slot, sizeof(ItemState), cudaMemcpyDeviceToHost) != cudaSuccess) return false;
+    if (!h.rel_buf || h.n_rel > h.rel_cap) return false;
+    out->resize(h.n_rel);
+    if (h.n_rel &&
+        cudaMemcpy(out->data(), h.rel_buf, h.n_rel * sizeof(RawRelation), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return false;
+    std::sort(out->begin(), out->end(), [](const RawRelation& a, const RawRelation& b) { return a.p < b.p; });
+    return true;
 }
 
 void serve_route(mps_server* sv, int k, std::vector<RawRelation>& rel, const WaveSlot& w) {
@@ -730,8 +878,23 @@ void serve_route(mps_server* sv, int k, std::vector<RawRelation>& rel, const Wav
             q.state = 2;
             q.t_done = std::chrono::steady_clock::now();
             std::sort(q.rel.begin(), q.rel.end(), [](const RawRelation& a, const RawRelation& b) { return a.p < b.p; });
+            // the item's device-resident result; it must equal the waves' host copy
+            std::vector<RawRelation> dev;
+            if (read_device_relations(sv, q, &dev)) {
+                const bool same = dev.size() == q.rel.size() &&
+                                  std::equal(dev.begin(), dev.end(), q.rel.begin(), [](const RawRelation& a, const RawRelation& b) {
+                                      return a.p == b.p && a.M == b.M && a.q == b.q;
+                                  });
+                if (same) {
+                    q.rel.swap(dev);
+                    q.relations_on_device = true;
+                } else {
+                    q.state = 3;
+                    q.error = MPS_E_STATE;
+                }
+            }
             sv->slot_owner[q.slot] = 0;
-            sv->mem_used -= q.mem;
+            sv->alloc.give(q.pool_off, q.mem);
             --sv->active;
         }
     }
@@ -754,18 +917,21 @@ void serve_loop(mps_server* sv) {
     mps_ctx* c = sv->ctx;
     cudaSetDevice(c->device);
     const u64 chunk = c->tun.chunk_odds;
+    // every wave of the server has one launch shape: the default configuration
+    // with the tables of the widest N range (launch_m_cap keeps every prime within them)
+    const BsgsCfg cfg = default_cfg(c);
     u32 tbits = 11;
     {
         u32 mb;
-        table_for(c, 10000000ull, &tbits, &mb);       // the widest N range sets the launch's table size
+        table_for(c, cfg, 10000000ull, &tbits, &mb);
     }
     int k = 0;
     std::unique_lock<std::mutex> lk(sv->mu);
     for (;;) {
-        // admission
+        // admission: an item enters when a device slot is free and its
+        // reservation fits in the pool; in arrival order
         while (!sv->queue.empty() && sv->active < sv->cfg.max_active) {
             ServeReq& q = sv->reqs[sv->queue.front()];
-            if (sv->active > 0 && sv->mem_used + q.mem > sv->cfg.mem_budget_bytes) break;
             int slot = -1;
             for (size_t i = 0; i < sv->slot_owner.size(); ++i)
                 if (sv->slot_owner[i] == 0) {
@@ -773,18 +939,33 @@ void serve_loop(mps_server* sv) {
                     break;
                 }
             if (slot < 0) break;
+            u64 off = 0;
+            if (!sv->alloc.take(q.mem, &off)) {
+                if (sv->active > 0) break;                  // waits until a reservation is released
+                // larger than the whole pool: it can never be admitted
+                sv->queue.pop_front();
+                q.state = 3;
+                q.error = MPS_E_CAPACITY;
+                q.t_done = std::chrono::steady_clock::now();
+                sv->cv_done.notify_all();
+                continue;
+            }
             sv->queue.pop_front();
             q.slot = slot;
+            q.pool_off = off;
             q.d.item_index = (u32)slot;
             sv->slot_owner[slot] = q.ticket;
-            sv->mem_used += q.mem;
             ++sv->active;
             q.state = 1;
             q.cursor = q.item.P0;
             q.t_admit = std::chrono::steady_clock::now();
             c->item_K[slot] = q.d.K;
+            c->item_cfg[slot] = cfg;
+            ItemState st{};
+            st.rel_cap = q.mem / sizeof(RawRelation);
+            st.rel_buf = reinterpret_cast<RawRelation*>(sv->pool + off);
             cudaError_t e = cudaMemcpy(c->d_items + slot, &q.d, sizeof(DevItem), cudaMemcpyHostToDevice);
-            if (e == cudaSuccess) e = cudaMemset(c->d_state + slot, 0, sizeof(ItemState));
+            if (e == cudaSuccess) e = cudaMemcpy(c->d_state + slot, &st, sizeof(ItemState), cudaMemcpyHostToDevice);
             if (e != cudaSuccess) {
                 serve_fail_all(sv, MPS_E_CUDA, std::string("item upload: ") + cudaGetErrorString(e));
                 break;
@@ -858,7 +1039,7 @@ void serve_loop(mps_server* sv) {
                 w.h_wave->runs[r].seg_begin = w.h_wave->total_segs;
                 w.h_wave->total_segs += (w.h_wave->runs[r].n_odds + kSieveSegOdds - 1) / kSieveSegOdds;
             }
-            const int r = slot_launch(c, w, tbits);
+            const int r = slot_launch(c, w, tbits, cfg);
             if (r) {
                 serve_fail_all(sv, r, c->err);
                 sv->cv_done.notify_all();
@@ -895,13 +1076,13 @@ int end_call(mps_ctx* c) {
 }
 
 // [lo, hi) in device chunks of at most chunk_odds odd numbers.
-int run_range(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, std::vector<RawRelation>& rel) {
+int run_range(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, const BsgsCfg& g, std::vector<RawRelation>& rel) {
     const u64 chunk = c->tun.chunk_odds;
     for (u64 a = lo; a < hi;) {
         const u64 lo_odd = std::max<u64>(a, 3) | 1ull;
         u64 b = hi;
         if (lo_odd < hi && (hi - lo_odd + 1) / 2 > chunk) b = lo_odd + 2 * chunk;
-        if (int r = run_chunk(c, a, b, item, K, rel)) return r;
+        if (int r = run_chunk(c, a, b, item, K, g, rel)) return r;
         a = b;
     }
     return MPS_OK;
@@ -909,11 +1090,12 @@ int run_range(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, std::vector<RawRelati
 
 int relations_of(mps_ctx* c, const mps_item* item, u64 lo, u64 hi, std::vector<RawRelation>& rel) {
     DevItem d;
-    if (int r = make_dev_item(c, item, 0, &d)) return r;
+    BsgsCfg g;
+    if (int r = make_dev_item(c, item, 0, &d, &g)) return r;
     if (lo >= hi) return MPS_OK;
     if (hi > kTwo62) return fail(c, MPS_E_RANGE, "hi must not exceed 2^62");
     if (int r = upload_items(c, &d, 1)) return r;
-    return run_range(c, lo, hi, 0, d.K, rel);
+    return run_range(c, lo, hi, 0, d.K, g, rel);
 }
 
 void sort_by_p(std::vector<RawRelation>& rel) {
@@ -987,6 +1169,8 @@ int mps_open(int device, const mps_tuning* tuning, mps_ctx** out) {
     if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "stream");
     for (cudaEvent_t* ev : {&c->ev0, &c->ev1, &c->evb0, &c->evb1})
         if ((e = cudaEventCreate(ev)) != cudaSuccess) return bail(e, "event");
+    for (cudaEvent_t& ev : c->evk)
+        if ((e = cudaEventCreate(&ev)) != cudaSuccess) return bail(e, "event");
     const HostTables& t = host_tables();
     const size_t n = t.sp.size();
     if ((e = cudaMalloc((void**)&c->d_sp, n * sizeof(u32))) != cudaSuccess) return bail(e, "tables");
@@ -997,6 +1181,7 @@ int mps_open(int device, const mps_tuning* tuning, mps_ctx** out) {
     if ((e = cudaMemcpy(c->d_sp, t.sp.data(), n * sizeof(u32), cudaMemcpyHostToDevice)) != cudaSuccess) return bail(e, "upload");
     if ((e = cudaMemcpy(c->d_rcp, t.rcp.data(), n * sizeof(u64), cudaMemcpyHostToDevice)) != cudaSuccess) return bail(e, "upload");
     if ((e = cudaMemcpy(c->d_inv, t.inv.data(), n * sizeof(u64), cudaMemcpyHostToDevice)) != cudaSuccess) return bail(e, "upload");
+    if (const char* cache = std::getenv("MPS_TUNE_CACHE")) mps_tune_load(c, cache);   // best effort
     *out = c;
     return MPS_OK;
 }
@@ -1012,6 +1197,8 @@ int mps_close(mps_ctx* c) {
     if (c->h_ctr) cudaFreeHost(c->h_ctr);
     if (c->h_rel) cudaFreeHost(c->h_rel);
     for (cudaEvent_t ev : {c->ev0, c->ev1, c->evb0, c->evb1})
+        if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : c->evk)
         if (ev) cudaEventDestroy(ev);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -1043,10 +1230,12 @@ int mps_item_relations(mps_ctx* c, const mps_item* item, mps_relation* out, size
     if (c && c->tun.plain) return mps_chunk_relations(c, item->P0, item->P1, item, out, cap, n_out);
     if (int r = check_ctx(c)) return r;
     DevItem d;
-    if (int r = make_dev_item(c, item, 0, &d)) return r;
+    BsgsCfg g;
+    if (int r = make_dev_item(c, item, 0, &d, &g)) return r;
     begin_call(c);
     std::vector<RawRelation> rel;
     c->item_K.assign(1, d.K);
+    c->item_cfg.assign(1, g);
     if (int r = upload_items(c, &d, 1)) return r;
     if (int r = run_waves(c, {item->P0}, {item->P1}, rel)) return r;
     if (int r = end_call(c)) return r;
@@ -1075,7 +1264,8 @@ int mps_filter(mps_ctx* c, const uint64_t* primes, size_t n, const mps_item* ite
     if (n == 0) return MPS_OK;
     if (!primes || !flags) return fail(c, MPS_E_ARG, "NULL buffer");
     DevItem d;
-    if (int r = make_dev_item(c, item, 0, &d)) return r;
+    BsgsCfg g;
+    if (int r = make_dev_item(c, item, 0, &d, &g)) return r;
     for (size_t i = 0; i < n; ++i)
         if (primes[i] >= kTwo62) return fail(c, MPS_E_RANGE, "primes must be below 2^62");
     begin_call(c);
@@ -1088,8 +1278,8 @@ int mps_filter(mps_ctx* c, const uint64_t* primes, size_t n, const mps_item* ite
         if (int r = ensure(c, &c->d_ent, &c->ent_cap, std::max<u64>(cnt, 1 << 16), "entry buffer")) return r;
         if (int r = ensure_rel(c, std::max<u64>(c->rel_cap, 1 << 18))) return r;
         u32 tbits, mb;
-        table_for(c, d.K, &tbits, &mb);
-        const u32 warps = c->tun.bsgs_warps;
+        table_for(c, g, d.K, &tbits, &mb);
+        const u32 warps = g.warps;
         int bgrid = 0;
         if (int r = bsgs_grid(c, tbits, warps, &bgrid)) return r;
         cudaStream_t s = c->stream;
@@ -1101,9 +1291,11 @@ int mps_filter(mps_ctx* c, const uint64_t* primes, size_t n, const mps_item* ite
         PrepArgs pa{};
         pa.surv = c->d_surv; pa.surv_cap = c->surv_cap; pa.item0 = 0; pa.items = c->d_items;
         pa.ent = c->d_ent; pa.ent_cap = c->ent_cap; pa.rel = c->d_rel; pa.rel_cap = c->rel_cap; pa.full_mr = c->tun.full_mr;
+        pa.m_cap = launch_m_cap(c, g, tbits);
         BsgsArgs ba{};
         ba.ent = c->d_ent; ba.ent_cap = c->ent_cap; ba.rel = c->d_rel; ba.rel_cap = c->rel_cap;
-        ba.tbits = tbits; ba.warps_per_block = warps; ba.persistent = 1; ba.chains = 2; ba.table_kind = c->tun.table_kind;
+        ba.tbits = tbits; ba.warps_per_block = warps; ba.persistent = 1; ba.chains = g.chains; ba.table_kind = g.kind;
+        ba.load_shift = g.load_shift;
         ba.max_p = *std::max_element(primes + off, primes + off + cnt);
         OrderArgs oa{};
         oa.rel = c->d_rel; oa.rel_cap = c->rel_cap; oa.items = c->d_items; oa.tables = c->tables();
@@ -1138,17 +1330,19 @@ int mps_batch_relations(mps_ctx* c, const mps_item* items, size_t n_items, mps_r
     if (int r = check_ctx(c)) return r;
     if (!items && n_items) return fail(c, MPS_E_ARG, "items is NULL");
     std::vector<DevItem> d(n_items);
+    std::vector<BsgsCfg> cfg(n_items);
     for (size_t i = 0; i < n_items; ++i)
-        if (int r = make_dev_item(c, &items[i], (u32)i, &d[i])) return r;
+        if (int r = make_dev_item(c, &items[i], (u32)i, &d[i], &cfg[i])) return r;
     begin_call(c);
     std::vector<RawRelation> rel;
     c->item_K.assign(n_items, 0);
     for (size_t i = 0; i < n_items; ++i) c->item_K[i] = d[i].K;
+    c->item_cfg = cfg;
     if (int r = upload_items(c, d.data(), n_items)) return r;
     if (c->tun.plain) {
         // the plain path: one item after another, one chunk at a time
         for (size_t i = 0; i < n_items; ++i)
-            if (int r = run_range(c, items[i].P0, items[i].P1, (u32)i, d[i].K, rel)) return r;
+            if (int r = run_range(c, items[i].P0, items[i].P1, (u32)i, d[i].K, cfg[i], rel)) return r;
     } else {
         std::vector<u64> lo(n_items), hi(n_items);
         for (size_t i = 0; i < n_items; ++i) {
@@ -1198,14 +1392,29 @@ int mps_serve_open(int device, const mps_tuning* tuning, const mps_serve_config*
         return r;
     }
     c->item_K.assign(conf.max_active, 0);
+    c->item_cfg.assign(conf.max_active, default_cfg(c));
     for (WaveSlot& w : c->slot)
         if (int r = slot_alloc(c, w)) {
             mps_close(c);
             return r;
         }
     c->slots_ready = true;
+    // the reservation pool: the budget, at most 90% of the device memory still free
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        mps_close(c);
+        return MPS_E_CUDA;
+    }
+    const u64 pool_bytes = std::min<u64>(conf.mem_budget_bytes, (u64)(0.9 * (double)free_b)) & ~255ull;
+    unsigned char* pool = nullptr;
+    if (pool_bytes < 4096 || cudaMalloc((void**)&pool, pool_bytes) != cudaSuccess) {
+        mps_close(c);
+        return MPS_E_CUDA;
+    }
     mps_server* sv = new mps_server();
     sv->ctx = c;
+    sv->pool = pool;
+    sv->alloc.reset(pool_bytes);
     sv->cfg = conf;
     sv->slot_owner.assign(conf.max_active, 0);
     sv->worker = std::thread(serve_loop, sv);
@@ -1222,7 +1431,7 @@ int mps_serve_submit(mps_server* sv, const mps_item* item, uint64_t* ticket) {
     if (sv->stop) return MPS_E_STATE;
     q.ticket = sv->next_ticket++;
     q.item = *item;
-    q.mem = item_memory(sv, q.d, *item);
+    q.mem = expected_relations(q.d, *item) * sizeof(RawRelation);
     q.t_submit = std::chrono::steady_clock::now();
     *ticket = q.ticket;
     sv->reqs[q.ticket] = std::move(q);
@@ -1248,6 +1457,8 @@ int mps_serve_wait(mps_server* sv, uint64_t ticket, double timeout_s, mps_serve_
         st->error = q.error;
         st->relations = q.rel.size();
         st->p_done = q.cursor;
+        st->reserved_bytes = q.mem;
+        st->relations_on_device = q.relations_on_device ? 1 : 0;
         if (q.state >= 2) {
             st->latency_ms = ms_between(q.t_submit, q.t_done);
             st->queue_ms = q.slot >= 0 || q.state == 2 ? ms_between(q.t_submit, q.t_admit) : 0.0;
@@ -1281,6 +1492,16 @@ int mps_serve_release(mps_server* sv, uint64_t ticket) {
     if (it == sv->reqs.end()) return MPS_E_ARG;
     if (it->second.state < 2) return MPS_E_STATE;
     sv->reqs.erase(it);
+    return MPS_OK;
+}
+
+int mps_serve_pool(mps_server* sv, uint64_t* pool_bytes, uint64_t* reserved_bytes, uint32_t* active, uint32_t* queued) {
+    if (!sv) return MPS_E_ARG;
+    std::lock_guard<std::mutex> g(sv->mu);
+    if (pool_bytes) *pool_bytes = sv->alloc.total();
+    if (reserved_bytes) *reserved_bytes = sv->alloc.used();
+    if (active) *active = sv->active;
+    if (queued) *queued = (uint32_t)sv->queue.size();
     return MPS_OK;
 }
 
@@ -1326,6 +1547,10 @@ int mps_serve_close(mps_server* sv) {
         sv->cv_work.notify_all();
     }
     if (sv->worker.joinable()) sv->worker.join();
+    if (sv->pool) {
+        cudaSetDevice(sv->ctx->device);
+        cudaFree(sv->pool);
+    }
     mps_close(sv->ctx);
     delete sv;
     return MPS_OK;
@@ -1384,6 +1609,162 @@ int mps_measure_peaks(mps_ctx* c, double* fmul_per_s, double* mmul_per_s, double
     if (fmul_per_s) *fmul_per_s = ops / (ms[0] * 1e-3);
     if (mmul_per_s) *mmul_per_s = ops / (ms[1] * 1e-3);
     if (imad_per_s) *imad_per_s = ops * 8.0 / (ms[2] * 1e-3);
+    return MPS_OK;
+}
+
+int mps_autotune(mps_ctx* c, const mps_item* items, size_t n_items, mps_tune_report* out, size_t cap,
+                 size_t* n_out) {
+    if (int r = check_ctx(c)) return r;
+    if (!items && n_items) return fail(c, MPS_E_ARG, "items is NULL");
+    if (!out && cap) return fail(c, MPS_E_ARG, "out is NULL");
+    constexpr u64 kCalibSpan = 1ull << 25;
+    const BsgsCfg base = default_cfg(c);
+    std::vector<BsgsCfg> cands{base};
+    for (u32 kind : {0u, 2u})
+        for (u32 ls : {2u, 3u}) {
+            if (kind != 2 && ls != 2) continue;
+            for (u32 ch : {1u, 2u, 4u})
+                for (u32 w : {4u, 8u}) {
+                    BsgsCfg g;
+                    g.kind = kind;
+                    g.load_shift = kind == 2 ? ls : base.load_shift;
+                    g.chains = ch;
+                    g.warps = w;
+                    if (g != base) cands.push_back(g);
+                }
+        }
+    std::vector<mps_tune_report> reps;
+    std::set<u64> seen;
+    for (size_t i = 0; i < n_items; ++i) {
+        DevItem d;
+        const char* why = "";
+        if (int r = item_constants(&items[i], c->tun.class_modulus, 0, &d, &why)) return fail(c, r, why);
+        const u64 key = tune_key(d.K, d.cm, items[i].P0);
+        if (!seen.insert(key).second || !d.has_work) continue;
+        const u64 lo = items[i].P0, hi = std::min<u64>(items[i].P1, items[i].P0 + kCalibSpan);
+        double best_ms = 0, base_ms = 0;
+        u64 entries = 0;
+        BsgsCfg best = base;
+        std::vector<RawRelation> first;
+        for (size_t k = 0; k < cands.size(); ++k) {
+            const BsgsCfg& g = cands[k];
+            u32 tb, mb;
+            table_for(c, g, d.K, &tb, &mb);
+            d.max_baby = mb;
+            if (bsgs_smem_bytes(tb, g.warps) > c->smem_optin) continue;
+            if (int r = upload_items(c, &d, 1)) return r;
+            double ms = 0;
+            for (int rep = 0; rep < 2; ++rep) {                 // the second run is timed
+                std::vector<RawRelation> rel;
+                std::memset(&c->stats, 0, sizeof(c->stats));
+                if (int r = run_chunk(c, lo, hi, 0, d.K, g, rel)) return r;
+                ms = c->stats.bsgs_ms;
+                entries = c->stats.entries;
+                sort_by_p(rel);
+                if (k == 0 && rep == 0) {
+                    first = rel;
+                } else if (rel.size() != first.size() ||
+                           !std::equal(rel.begin(), rel.end(), first.begin(), [](const RawRelation& a, const RawRelation& b) {
+                               return a.p == b.p && a.M == b.M && a.q == b.q;
+                           })) {
+                    return fail(c, MPS_E_CUDA, "tuning candidates gave different relations");
+                }
+            }
+            if (k == 0) base_ms = ms;
+            if (k == 0 || ms < best_ms) {
+                best_ms = ms;
+                best = g;
+            }
+        }
+        const double per = entries ? 1e6 / (double)entries : 0.0;
+        TuneEntry te;
+        te.cfg = best;
+        te.ns_per_prime = best_ms * per;
+        c->tuned[key] = te;
+        mps_tune_report rp{};
+        rp.k_bits = (u32)(key >> 40);
+        rp.mod = (u32)((key >> 8) & 4095);
+        rp.p_digits = (u32)(key & 255);
+        rp.candidates = (u32)cands.size();
+        rp.table_kind = best.kind;
+        rp.load_shift = best.load_shift;
+        rp.chains = best.chains;
+        rp.warps = best.warps;
+        rp.best_ns_per_prime = best_ms * per;
+        rp.default_ns_per_prime = base_ms * per;
+        rp.calib_bsgs_primes = entries;
+        reps.push_back(rp);
+    }
+    std::memset(&c->stats, 0, sizeof(c->stats));
+    if (n_out) *n_out = reps.size();
+    if (reps.size() > cap) return fail(c, MPS_E_CAPACITY, "report buffer too small");
+    for (size_t k = 0; k < reps.size(); ++k) out[k] = reps[k];
+    return MPS_OK;
+}
+
+int mps_tune_save(const mps_ctx* c, const char* path) {
+    if (!c || !path) return MPS_E_ARG;
+    FILE* f = std::fopen(path, "w");
+    if (!f) return MPS_E_ARG;
+    std::fprintf(f, "mps-tune 1\n");
+    for (const auto& kv : c->tuned)
+        std::fprintf(f, "%llu %u %u %u %u %.3f\n", (unsigned long long)kv.first, kv.second.cfg.kind,
+                     kv.second.cfg.load_shift, kv.second.cfg.chains, kv.second.cfg.warps, kv.second.ns_per_prime);
+    return std::fclose(f) == 0 ? MPS_OK : MPS_E_ARG;
+}
+
+int mps_tune_load(mps_ctx* c, const char* path) {
+    if (!c || !path) return MPS_E_ARG;
+    FILE* f = std::fopen(path, "r");
+    if (!f) return fail(c, MPS_E_ARG, std::string("cannot open ") + path);
+    char head[32] = {0};
+    if (!std::fgets(head, sizeof(head), f) || std::strncmp(head, "mps-tune 1", 10) != 0) {
+        std::fclose(f);
+        return fail(c, MPS_E_ARG, "not a tuning file");
+    }
+    unsigned long long key;
+    unsigned kind, ls, ch, w;
+    double ns;
+    while (std::fscanf(f, "%llu %u %u %u %u %lf", &key, &kind, &ls, &ch, &w, &ns) == 6) {
+        // only configurations the kernels are built for
+        if (kind > 2 || ls < 1 || ls > 4 || (ch != 1 && ch != 2 && ch != 4) || w < 1 || w > 8) continue;
+        TuneEntry te;
+        te.cfg.kind = kind;
+        te.cfg.load_shift = ls;
+        te.cfg.chains = ch;
+        te.cfg.warps = w;
+        te.ns_per_prime = ns;
+        c->tuned[key] = te;
+    }
+    std::fclose(f);
+    return MPS_OK;
+}
+
+int mps_tune_clear(mps_ctx* c) {
+    if (!c) return MPS_E_ARG;
+    c->tuned.clear();
+    return MPS_OK;
+}
+
+int mps_measure_smem_peak(mps_ctx* c, double* atomic_or_per_s) {
+    if (int r = check_ctx(c)) return r;
+    if (!atomic_or_per_s) return fail(c, MPS_E_ARG, "NULL output");
+    u32* sink = nullptr;
+    CK(cudaMalloc((void**)&sink, 64), "alloc");
+    const int grid = c->num_sms * 8;
+    const u32 iters = 2048;
+    float ms = 0;
+    cudaError_t e = cudaSuccess;
+    for (int rep = 0; rep < 2 && e == cudaSuccess; ++rep) {     // the second repetition is kept
+        e = cudaEventRecord(c->ev0, c->stream);
+        if (e == cudaSuccess) e = launch_smem_or_peak(iters, grid, sink, c->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(c->ev1, c->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(c->ev1);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    }
+    cudaFree(sink);
+    if (e != cudaSuccess) return cuda_fail(c, e, "shared-memory probe");
+    *atomic_or_per_s = (double)grid * 256.0 * 8.0 * iters / (ms * 1e-3);
     return MPS_OK;
 }
 

@@ -43,6 +43,11 @@ struct DevItem {
     u32 item_index;
     u32 qf_n;              // prime factors of Q: qf_l[0..qf_n)
     u32 qf_l[7];
+    // Quadratic-character prefilter (both |b| and |c| below 2^32): for x = b
+    // and x = -c, x = (-1)^neg 2^k o with o odd; rcp = floor((2^64-1) / o).
+    u32 qr_on;
+    u32 qr_neg[2], qr_k[2], qr_o[2];
+    u64 qr_rcp[2];
 };
 
 // One prime that reached the discrete-log stage: solve G0 * B^j == t (mod p)

@@ -20,6 +20,9 @@
 #include "arith.cuh"
 #include "mps_kernels.cuh"
 
+#include <algorithm>
+#include <mutex>
+
 namespace mps {
 
 constexpr u32 FULL = 0xFFFFFFFFu;
@@ -359,6 +362,22 @@ __device__ __forceinline__ bool prep_special(u64 p, const DevItem& it, const Pre
     return t != 0 && it.has_work;
 }
 
+// Quadratic-character prefilter (the reference's Jacobi filter, Gpu.hpp:
+// 247-263, restated): b^n == t (mod p) forces (b/p)^n == (t/p).  With every
+// in-class n == n_start (mod cm): for even cm the parity of n is fixed, so
+// (b/p)^(n_start mod 2) must equal (t/p); for odd cm, (b/p) = 1 forces
+// (t/p) = 1.  True when p can be dropped: a prime p then has no in-class
+// solution, and a composite p never gives a relation.  Costs two Jacobi
+// symbols of 32-bit numbers, before any modular exponentiation.
+__device__ __forceinline__ bool qr_reject(u64 p, const DevItem& it) {
+    if (!it.qr_on) return false;
+    const int jb = jacobi_small(p, it.qr_neg[0], it.qr_k[0], it.qr_o[0], it.qr_rcp[0]);
+    const int jt = jacobi_small(p, it.qr_neg[1], it.qr_k[1], it.qr_o[1], it.qr_rcp[1]);
+    if (jb == 0 || jt == 0) return false;              // p shares a factor with b or c: the exact path decides
+    if ((it.cm & 1) == 0) return (it.n_start & 1) ? jb != jt : jt != 1;
+    return jb == 1 && jt != 1;
+}
+
 // e = (p - 1) / g exactly, g | p - 1.
 __device__ __forceinline__ u64 exact_quotient(u64 pm1, u32 g) {
     const int tz = __ffs(g) - 1;
@@ -488,6 +507,7 @@ __device__ void bsgs_setup(const F& f, u64 p, u64 b_mod, u64 t, const DevItem& i
     const V Bv = f.pow(bv, L);
     u32 m = (u32)isqrt_ceil_dev(jcount);
     if (m > it.max_baby) m = it.max_baby;
+    if (m > a.m_cap) m = a.m_cap;                      // never more than the launch's tables hold
     const u64 Bm = f.residue(f.pow(Bv, m));
     const u64 slot = atomicAdd(&ctr->entries, 1ull);
     if (slot >= a.ent_cap) {
@@ -552,7 +572,7 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep(PrepArgs a, Counters* ctr
                 p = a.surv[b0 + k];
                 if (a.surv_item) item = a.surv_item[b0 + k];
                 u64 bm, t;
-                if (prep_special(p, a.items[item], a, ctr, bm, t))
+                if (prep_special(p, a.items[item], a, ctr, bm, t) && !qr_reject(p, a.items[item]))
                     keep = p < kFp64Limit ? stage1<FieldF>(p, a) : stage1<FieldM>(p, a);
             }
             const u32 s = queue_slot(&n_q, keep);
@@ -1187,10 +1207,181 @@ __device__ u64 solve_fp64q(const Entry& e, unsigned long long* tab, u32 tbits, u
     return best < e.jcount ? best : ~0ull;
 }
 
+// ---- the FP64 solve with a 16-bit slot table ----
+//
+// Table: 2^(tbits+1) 16-bit slots per warp (4 << tbits bytes), of which a
+// prime with m baby steps uses 2^tw, tw = ceil(log2 m) + load_shift (load at
+// most 2^-load_shift).  A key -- the canonical residue x of a baby step -- is
+// hashed from the low 32 bits of x, which the FP64 pipe exposes with one add
+// (x + 2^52 has x in its low mantissa bits): h = lo32(x) * kHashMul, a
+// bijection of lo32(x).  The home slot is the top tw bits of h and holds the
+// 15-bit fingerprint (h & 0x7FFF) | 1 (never 0; 0 is an empty slot).  Bit 15
+// of a slot is its overflow flag, set when a key homed there found it taken
+// and moved on (linear probing).  A probe reads its home slot only: equal
+// fingerprints make a candidate; a set overflow flag sends the lane to the
+// warp's slow path, which walks the chain.  Candidates are resolved exactly by
+// recomputing the baby steps, so fingerprint collisions (about 2^-14 per
+// occupied probe) never change a result.
+
+constexpr u32 kHashMul = 0x9E3779B1u;
+
+__device__ __forceinline__ u32 hkey_canon(double x) {          // x canonical in [0, p), p < 2^49
+    return (u32)__double2loint(__dadd_rn(x, 4503599627370496.0)) * kHashMul;
+}
+
+__device__ __forceinline__ u32 hfp(u32 h) { return (h & 0x7FFFu) | 1u; }
+
+__device__ __forceinline__ void h_insert(unsigned short* tab, u32 mask, u32 shift, u32 h) {
+    u32 s = h >> shift;
+    const unsigned short f = (unsigned short)hfp(h);
+    if (atomicCAS(&tab[s], (unsigned short)0, f) == 0) return;
+    atomicOr(reinterpret_cast<u32*>(tab) + (s >> 1), 0x8000u << (16 * (s & 1)));   // flag the home slot
+    do s = (s + 1) & mask;
+    while (atomicCAS(&tab[s], (unsigned short)0, f) != 0);
+}
+
+// Whether a key with hash h may be in the table: its home slot, then (when the
+// home's overflow flag is set) the chain up to the first empty slot.
+__device__ __forceinline__ bool h_contains(const unsigned short* tab, u32 mask, u32 shift, u32 h) {
+    u32 s = h >> shift;
+    const u32 f = hfp(h);
+    u32 e = tab[s];
+    if (((e ^ f) & 0x7FFFu) == 0) return true;
+    if (!(e & 0x8000u)) return false;
+    for (u32 n = 0; n < mask; ++n) {
+        s = (s + 1) & mask;
+        e = tab[s];
+        if (e == 0) return false;
+        if (((e ^ f) & 0x7FFFu) == 0) return true;
+    }
+    return false;
+}
+
+template <int CH>
+__device__ u64 solve_fp64h(const Entry& e, unsigned short* tab, u32 tbits, u32 load_shift, u64* steps_out) {
+    const u32 lane = threadIdx.x & 31;
+    Fp64 f;
+    f.init(e.p);
+    const u32 m = e.m;
+    const u32 jc = (u32)e.jcount;                      // jcount <= 10^7
+    const u32 tw = min(tbits + 1, max(6u, 32u - __clz(max(m, 2u) - 1) + load_shift));
+    const u32 mask = (1u << tw) - 1, shift = 32 - tw;
+    const double B = (double)e.B, Bm = (double)e.Bm, tv = (double)e.t, G0 = (double)e.G0;
+
+    double xb = B, xg = Bm;                            // B^(l+1), Bm^(l+1)
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const double yb = __shfl_up_sync(FULL, xb, off), yg = __shfl_up_sync(FULL, xg, off);
+        if (lane >= (u32)off) {
+            xb = f.mul(xb, yb);
+            xg = f.mul(xg, yg);
+        }
+    }
+    const double B32 = __shfl_sync(FULL, xb, 31), Bm32 = __shfl_sync(FULL, xg, 31);
+    double bl = __shfl_up_sync(FULL, xb, 1);
+    if (lane == 0) bl = 1.0;
+    double Bstep = B32, Gstep = Bm32;                  // B^(32 CH), Bm^(32 CH)
+#pragma unroll
+    for (int c = 1; c < CH; c <<= 1) {
+        Bstep = f.mul(Bstep, Bstep);
+        Gstep = f.mul(Gstep, Gstep);
+    }
+    const double tbl = f.mul(tv, bl);
+    double bx[CH], gx[CH];
+    bx[0] = tbl;
+    gx[0] = f.mul(G0, xg);
+#pragma unroll
+    for (int c = 1; c < CH; ++c) {
+        bx[c] = f.mul(bx[c - 1], B32);
+        gx[c] = f.mul(gx[c - 1], Bm32);
+    }
+
+    uint4* t4 = reinterpret_cast<uint4*>(tab);
+    for (u32 k = lane; k <= (mask >> 3); k += 32) t4[k] = make_uint4(0, 0, 0, 0);
+    __syncwarp();
+
+    // baby steps, stopping at a cycle B^d == 1 (d < m)
+    u32 cyc = 0, baby_done = m;
+    for (u32 base = 0; base < m; base += 32 * CH) {
+        double cv[CH];
+        u32 cb = 0;
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            cv[c] = f.canon(bx[c]);
+            const u32 i = base + 32 * c + lane;
+            const u32 bc = __ballot_sync(FULL, i > 0 && i < m && cv[c] == tv);
+            if (bc && !cb) cb = base + 32 * c + __ffs(bc) - 1;
+        }
+        const u32 lim = cb ? cb : m;
+#pragma unroll
+        for (int c = 0; c < CH; ++c)
+            if (base + 32 * c + lane < lim) h_insert(tab, mask, shift, hkey_canon(cv[c]));
+        if (cb) {
+            cyc = cb;
+            baby_done = cb;
+            break;
+        }
+#pragma unroll
+        for (int c = 0; c < CH; ++c) bx[c] = f.mul(bx[c], Bstep);
+    }
+    __syncwarp();
+
+    u64 best = ~0ull;
+    u32 giant_done = 0;
+    if (cyc) {
+        const int i = ffind_baby(f, tbl, B32, 1, cyc, G0);
+        if (i > 0) best = cyc - (u32)i;
+    } else {
+        const u32 G = (jc - 1 + m - 1) / m;            // g = 1..G covers j in [1, G*m]
+        giant_done = G;
+        for (u32 base = 0; base < G; base += 32 * CH) {
+            u32 hs[CH];
+            bool flag = false;
+#pragma unroll
+            for (int c = 0; c < CH; ++c) {
+                hs[c] = hkey_canon(f.canon(gx[c]));
+                const u32 slot = tab[hs[c] >> shift];
+                flag |= (((slot ^ hfp(hs[c])) & 0x7FFFu) == 0) | ((slot & 0x8000u) != 0);
+            }
+            if (__any_sync(FULL, flag)) {
+                // the slow path: walk overflowed homes, then resolve candidates in increasing g
+                u32 real = 0;
+#pragma unroll
+                for (int c = 0; c < CH; ++c)
+                    if (base + 32 * c + lane + 1 <= G && h_contains(tab, mask, shift, hs[c])) real |= 1u << c;
+                u64 jb = ~0ull;
+#pragma unroll
+                for (int c = 0; c < CH; ++c) {
+                    u32 bb = __ballot_sync(FULL, (real >> c) & 1u);
+                    while (bb && jb == ~0ull) {
+                        const int src = __ffs(bb) - 1;
+                        bb &= bb - 1;
+                        const double v = __shfl_sync(FULL, f.canon(gx[c]), src);
+                        const u64 g = base + 32 * c + (u32)src + 1;
+                        const int i = ffind_baby(f, tbl, B32, 0, m, v);
+                        if (i >= 0) jb = g * m - (u64)i;
+                    }
+                }
+                if (jb != ~0ull) {
+                    best = jb;
+                    giant_done = min(G, base + 32 * CH);
+                    break;
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < CH; ++c) gx[c] = f.mul(gx[c], Gstep);
+        }
+    }
+    __syncwarp();
+    if (steps_out) *steps_out = (u64)baby_done + giant_done;
+    return best < e.jcount ? best : ~0ull;
+}
+
 template <int CH, int QT>
-__device__ __forceinline__ u64 solve_any(const Entry& e, void* tab, u32 tbits, u64* steps) {
+__device__ __forceinline__ u64 solve_any(const Entry& e, void* tab, u32 tbits, u32 load_shift, u64* steps) {
     if (CH == 0 || e.p >= kFp64Limit) return solve_entry<FieldM>(e, (unsigned short*)tab, tbits + 1, steps);
     if (QT == 0) return solve_fp64q<CH ? CH : 1>(e, (unsigned long long*)tab, tbits, steps);
+    if (QT == 2) return solve_fp64h<CH ? CH : 1>(e, (unsigned short*)tab, tbits, load_shift, steps);
     return solve_fp64<CH ? CH : 1>(e, (u32*)tab, tbits, steps);
 }
 
@@ -1211,7 +1402,7 @@ __global__ void __launch_bounds__(256, MPS_BSGS_MINB) k_bsgs(BsgsArgs a, Counter
             if (idx >= n_ent) break;
             const Entry e = a.ent[idx];
             u64 steps = 0;
-            const u64 j = solve_any<CH, QT>(e, tab, a.tbits, &steps);
+            const u64 j = solve_any<CH, QT>(e, tab, a.tbits, a.load_shift, &steps);
             if (lane == 0) {
                 if (j != ~0ull) emit_relation(e.p, e.n_first + j * e.L, 0, e.item, a.rel, a.rel_cap, ctr);
                 my_steps += steps;
@@ -1223,7 +1414,7 @@ __global__ void __launch_bounds__(256, MPS_BSGS_MINB) k_bsgs(BsgsArgs a, Counter
         if (idx >= n_ent) return;
         const Entry e = a.ent[idx];
         u64 steps = 0;
-        const u64 j = solve_any<CH, QT>(e, tab, a.tbits, &steps);
+        const u64 j = solve_any<CH, QT>(e, tab, a.tbits, a.load_shift, &steps);
         if (lane == 0) {
             if (j != ~0ull) emit_relation(e.p, e.n_first + j * e.L, 0, e.item, a.rel, a.rel_cap, ctr);
             atomicAdd(&ctr->steps, (unsigned long long)steps);
@@ -1388,7 +1579,10 @@ __global__ void __launch_bounds__(128) k_order(OrderArgs a, Counters* ctr) {
 
 // ------------------------------------------------------- served-item state --
 
+// A wave whose buffers overflowed commits nothing: the host redoes its runs
+// and records them with k_state_add.
 __global__ void k_commit(const WaveDesc* w, const RawRelation* rel, const Counters* ctr, u64 rel_cap, ItemState* st) {
+    if (ctr->status & (kStatusSurvivorOverflow | kStatusEntryOverflow | kStatusRelationOverflow)) return;
     const u32 tid = blockIdx.x * blockDim.x + threadIdx.x;
     const u32 n_runs = w->n_runs;
     if (tid < n_runs) {
@@ -1397,8 +1591,26 @@ __global__ void k_commit(const WaveDesc* w, const RawRelation* rel, const Counte
         atomicAdd(&st[r.item].waves, 1ull);
     }
     const u64 n = min((u64)ctr->relations, rel_cap);
-    for (u64 i = tid; i < n; i += (u64)gridDim.x * blockDim.x)
-        if (rel[i].q != ~0ull) atomicAdd(&st[rel[i].item].n_rel, 1ull);
+    for (u64 i = tid; i < n; i += (u64)gridDim.x * blockDim.x) {
+        const RawRelation r = rel[i];
+        if (r.q == ~0ull) continue;                     // a composite survivor
+        ItemState& s = st[r.item];
+        const u64 k = atomicAdd(&s.n_rel, 1ull);
+        if (s.rel_buf && k < s.rel_cap) s.rel_buf[k] = r;
+    }
+}
+
+// One run redone on the host path: advance the item to hi, append its relations.
+__global__ void k_state_add(ItemState* st, u32 item, u64 hi, const RawRelation* rel, u64 n) {
+    ItemState& s = st[item];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicMax(&s.p_done, (unsigned long long)hi);
+        atomicAdd(&s.waves, 1ull);
+    }
+    for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        const u64 k = atomicAdd(&s.n_rel, 1ull);
+        if (s.rel_buf && k < s.rel_cap) s.rel_buf[k] = rel[i];
+    }
 }
 
 // ------------------------------------------------------ prime counting --
@@ -1506,6 +1718,22 @@ __global__ void __launch_bounds__(256) k_imad_peak(u32 iters, u32* sink) {
     if (acc == 0x12345u) sink[0] = acc;
 }
 
+// Conflict-free shared-memory atomicOr: lane l of every warp always hits
+// bank l of an 8 KB bitmap (the sieve's segment), 8 independent words per
+// thread per iteration.
+__global__ void __launch_bounds__(256) k_smem_or_peak(u32 iters, u32* sink) {
+    __shared__ u32 bits[kSegWords];
+    const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (u32 w = threadIdx.x; w < kSegWords; w += blockDim.x) bits[w] = 0;
+    __syncthreads();
+    for (u32 i = 0; i < iters; ++i) {
+#pragma unroll
+        for (u32 k = 0; k < 8; ++k) atomicOr(&bits[lane + 32 * ((warp * 8 + k + i) & 63)], 1u << ((i + k) & 31));
+    }
+    __syncthreads();
+    if (bits[threadIdx.x] == 0x12345u) sink[0] = bits[threadIdx.x];
+}
+
 // ------------------------------------------------------------- test hooks --
 
 __global__ void k_is_prime(const u64* n, u32* out, u64 count) {
@@ -1533,16 +1761,19 @@ __global__ void k_bsgs_direct(const u64* cases, u64* j_out, u64 count, u32 tbits
     } else {
         u32 m = (u32)isqrt_ceil_dev(e.jcount);
         // the table loads of the sieving path
-        const u32 cap = min(kMaxBaby, table_kind == 0 ? 1u << (tbits - 1) : max(1u, (1u << tbits) / 5));
+        const u32 cap = min(kMaxBaby, table_kind == 0   ? 1u << (tbits - 1)
+                                      : table_kind == 2 ? 1u << (tbits + 1 - kDefaultLoadShift)
+                                                        : max(1u, (1u << tbits) / 5));
         if (m > cap) m = cap;
         e.m = m;
         Mont M;
         M.init(p);
         const u64 rr = M.r2();
         e.Bm = M.from_mont(M.pow(M.to_mont(e.B, rr), m));
-        if (e.p >= kFp64Limit) result = solve_any<0, 0>(e, smem32, tbits, nullptr);
-        else if (table_kind == 0) result = solve_any<2, 0>(e, smem32, tbits, nullptr);
-        else result = solve_any<2, 1>(e, smem32, tbits, nullptr);
+        if (e.p >= kFp64Limit) result = solve_any<0, 0>(e, smem32, tbits, kDefaultLoadShift, nullptr);
+        else if (table_kind == 0) result = solve_any<2, 0>(e, smem32, tbits, kDefaultLoadShift, nullptr);
+        else if (table_kind == 2) result = solve_any<2, 2>(e, smem32, tbits, kDefaultLoadShift, nullptr);
+        else result = solve_any<2, 1>(e, smem32, tbits, kDefaultLoadShift, nullptr);
     }
     if (threadIdx.x == 0) j_out[idx] = result;
 }
@@ -1581,17 +1812,25 @@ cudaError_t launch_prep(const PrepArgs& a, Counters* ctr, int grid, cudaStream_t
     return cudaGetLastError();
 }
 
-// Dynamic shared memory limit of every k_bsgs variant (set once per size,
-// before any graph capture; a set during capture is not needed then).
+// Dynamic shared memory limit of every k_bsgs variant on the current device
+// (the attribute is per device; set once per size and device, before any
+// graph capture, so that a captured launch never needs it).
 cudaError_t bsgs_reserve_smem(size_t smem) {
-    static size_t done = 0;
-    if (smem <= done) return cudaSuccess;
+    constexpr int kDevices = 64;
+    static std::mutex lock;
+    static size_t done[kDevices] = {};
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) return err;
+    if (dev < 0 || dev >= kDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> g(lock);
+    if (smem <= done[dev]) return cudaSuccess;
     for (auto kern : {k_bsgs<0, 0>, k_bsgs<1, 0>, k_bsgs<2, 0>, k_bsgs<4, 0>, k_bsgs<1, 1>, k_bsgs<2, 1>,
-                      k_bsgs<4, 1>}) {
-        cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                      k_bsgs<4, 1>, k_bsgs<1, 2>, k_bsgs<2, 2>, k_bsgs<4, 2>}) {
+        err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (err != cudaSuccess) return err;
     }
-    done = smem;
+    done[dev] = smem;
     return cudaSuccess;
 }
 
@@ -1604,6 +1843,11 @@ cudaError_t launch_bsgs(const BsgsArgs& a, Counters* ctr, int grid, cudaStream_t
         return cudaGetLastError();
     };
     if (a.max_p >= kFp64Limit) return go(k_bsgs<0, 0>);
+    if (a.table_kind == 2) {
+        if (a.chains == 4) return go(k_bsgs<4, 2>);
+        if (a.chains == 1) return go(k_bsgs<1, 2>);
+        return go(k_bsgs<2, 2>);
+    }
     if (a.table_kind == 1) {
         if (a.chains == 4) return go(k_bsgs<4, 1>);
         if (a.chains == 1) return go(k_bsgs<1, 1>);
@@ -1625,6 +1869,11 @@ cudaError_t launch_commit(const WaveDesc* w, const RawRelation* rel, const Count
     return cudaGetLastError();
 }
 
+cudaError_t launch_state_add(ItemState* st, u32 item, u64 hi, const RawRelation* rel, u64 n, cudaStream_t s) {
+    k_state_add<<<(unsigned)std::min<u64>((n + 255) / 256 + 1, 256), 256, 0, s>>>(st, item, hi, rel, n);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_count_primes(const u64* surv, u64 surv_cap, Counters* ctr, int grid, cudaStream_t s) {
     k_count_primes<<<grid, 256, 0, s>>>(surv, surv_cap, ctr);
     return cudaGetLastError();
@@ -1642,6 +1891,11 @@ cudaError_t launch_fmul_peak(u64 p, u32 iters, int grid, u64* sink, cudaStream_t
 
 cudaError_t launch_imad_peak(u32 iters, int grid, u32* sink, cudaStream_t s) {
     k_imad_peak<<<grid, 256, 0, s>>>(iters, sink);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_smem_or_peak(u32 iters, int grid, u32* sink, cudaStream_t s) {
+    k_smem_or_peak<<<grid, 256, 0, s>>>(iters, sink);
     return cudaGetLastError();
 }
 

@@ -41,13 +41,17 @@ struct SieveRun {
     u32 pad;
 };
 
-// Device-resident progress of one served item: every P below p_done is
-// sieved once the wave that covered it has committed; n_rel relations found.
+// Device-resident state of one item: every P below p_done is sieved once the
+// wave that covered it has committed; n_rel relations found, the first rel_cap
+// of them kept in rel_buf (the item's reservation in a server's device pool;
+// nullptr when the relations are not kept on the device).
 struct ItemState {
     unsigned long long p_done;
     unsigned long long n_rel;
     unsigned long long waves;
-    unsigned long long pad;
+    unsigned long long rel_cap;
+    RawRelation* rel_buf;
+    unsigned long long pad[3];
 };
 struct WaveDesc {
     u32 n_runs;
@@ -59,6 +63,9 @@ constexpr u64 kSieveSegOdds = 65536;   // odd numbers per sieve segment (one blo
 // After a wave: advance each run's item to the run's end, count relations.
 cudaError_t launch_commit(const WaveDesc* w, const RawRelation* rel, const Counters* ctr, u64 rel_cap,
                           ItemState* st, cudaStream_t s);
+// A run of an overflowed wave, redone on the host path: p_done = max(p_done, hi),
+// its n relations rel[0..n) appended to the item's state.
+cudaError_t launch_state_add(ItemState* st, u32 item, u64 hi, const RawRelation* rel, u64 n, cudaStream_t s);
 cudaError_t launch_sieve_wave(const WaveDesc* w, const SieveTables& t, u64* surv, u32* surv_item, u64 surv_cap,
                               Counters* ctr, int grid, cudaStream_t s);
 
@@ -74,6 +81,7 @@ struct PrepArgs {
     RawRelation* rel;
     u64 rel_cap;
     u32 full_mr;               // 1: 12-base Miller-Rabin on every survivor that passes the filters
+    u32 m_cap;                 // baby steps per prime at most (what the launch's BSGS tables hold)
 };
 cudaError_t launch_prep(const PrepArgs& a, Counters* ctr, int grid, cudaStream_t s);
 
@@ -88,8 +96,10 @@ struct BsgsArgs {
     u32 persistent;            // 1: work-stealing warps; 0: one warp per entry
     u32 chains;                // FP64 solve: independent chains per lane (1, 2, 4)
     u64 max_p;                 // largest p of the entries (>= 2^49: integer solve)
-    u32 table_kind;            // FP64 solve: 0 = fingerprint words, 1 = 32-bit slots
+    u32 table_kind;            // FP64 solve: 0 = fingerprint words, 1 = 32-bit slots, 2 = 16-bit slots
+    u32 load_shift;            // table kind 2: at most 2^-load_shift of a prime's slots are used
 };
+constexpr u32 kDefaultLoadShift = 2;
 cudaError_t launch_bsgs(const BsgsArgs& a, Counters* ctr, int grid, cudaStream_t s);
 cudaError_t bsgs_reserve_smem(size_t smem);   // call before capturing a launch_bsgs
 
@@ -109,6 +119,7 @@ cudaError_t launch_count_primes(const u64* surv, u64 surv_cap, Counters* ctr, in
 cudaError_t launch_mmul_peak(u64 p, u32 iters, int grid, u64* sink, cudaStream_t s);
 cudaError_t launch_imad_peak(u32 iters, int grid, u32* sink, cudaStream_t s);
 cudaError_t launch_fmul_peak(u64 p, u32 iters, int grid, u64* sink, cudaStream_t s);
+cudaError_t launch_smem_or_peak(u32 iters, int grid, u32* sink, cudaStream_t s);   // 256 x grid x 8 x iters
 
 // Test hooks: raw kernels on given inputs.
 cudaError_t launch_is_prime(const u64* n, u32* out, u64 count, cudaStream_t s);

@@ -17,11 +17,16 @@
 // device (with that device current); make the first call before capturing
 // work on any stream into a CUDA graph.  Every call shares the one array and
 // leaves the previous call's contents in it: the counters are cleared at the
-// start of each pass.  Calls that overlap on the GPU (two host threads, or
-// two devices' worth of work on one device at once) race on the array and
-// must not be made.  No cudaMalloc, cudaFree, cudaMallocHost or other
-// allocating routine is called, on the device or the host.
+// start of each pass.  Calls that overlap on one GPU (two host threads
+// calling at once for the same device) race on that device's array and must
+// not be made; calls on different devices use different arrays and may
+// overlap.  The work is queued on the calling thread's per-thread default
+// stream (cudaStreamPerThread), so it neither waits for nor blocks other
+// streams of the device, and the host waits only for that stream.  No
+// cudaMalloc, cudaFree, cudaMallocHost or other allocating routine is called,
+// on the device or the host.
 #include "../../include/mps_gpu.h"
+#include "mps_item.cuh"
 #include "mps_kernels.cuh"
 
 #include <algorithm>
@@ -116,61 +121,17 @@ unsigned char* scratch_for_current_device(int* code) {
     return base;
 }
 
-u64 gcd_u64(u64 a, u64 b) {
-    while (b) {
-        const u64 t = a % b;
-        a = b;
-        b = t;
-    }
-    return a;
-}
-
-// The item's device constants with the default tuning (same rules as the
-// regular entry points: load_worktodo's checks plus P1 <= 2^62).
-int item_constants(const mps_item* it, DevItem* d, u32* tbits) {
-    if (!it) return MPS_E_ARG;
-    if (it->P0 >= it->P1 || it->N0 >= it->N1) return MPS_E_ARG;
-    if (it->P1 > (1ull << 62)) return MPS_E_RANGE;
-    if ((unsigned __int128)((__int128)it->N1 - it->N0) > 10000000ull) return MPS_E_RANGE;
-    const u64 cm = it->mod == 0 ? 1 : it->mod;
-    if (it->res >= cm) return MPS_E_ARG;
-    std::memset(d, 0, sizeof(*d));
-    const __int128 b = (__int128)(((unsigned __int128)(u64)it->b_hi << 64) | it->b_lo);
-    const __int128 c = (__int128)(((unsigned __int128)(u64)it->c_hi << 64) | it->c_lo);
-    const unsigned __int128 babs = b < 0 ? (unsigned __int128)0 - (unsigned __int128)b : (unsigned __int128)b;
-    const unsigned __int128 cabs = c < 0 ? (unsigned __int128)0 - (unsigned __int128)c : (unsigned __int128)c;
-    d->babs_hi = (u64)(babs >> 64);
-    d->babs_lo = (u64)babs;
-    d->cabs_hi = (u64)(cabs >> 64);
-    d->cabs_lo = (u64)cabs;
-    d->b_neg = b < 0;
-    d->c_neg = c < 0;
-    d->N0_raw = it->N0;
-    d->N1_raw = it->N1;
-    d->N0 = it->N0 < 0 ? 0 : (u64)it->N0;
-    d->N1 = it->N1 < 0 ? 0 : (u64)it->N1;
-    d->cm = cm;
-    d->n_start = d->N0 + ((it->res % cm) + cm - (d->N0 % cm)) % cm;
-    d->has_work = (it->N1 > 0 && d->n_start < d->N1) ? 1 : 0;
-    d->K = d->has_work ? (d->N1 - d->n_start + cm - 1) / cm : 0;
-    const u64 l = cm / gcd_u64(cm, 5040) * 5040;
-    const u64 Q = l <= 100800 ? l : 5040;
-    d->Q = (u32)Q;
-    d->Q_rcp = ~0ull / Q;
-    d->cmQ = (u32)(cm % Q);
-    d->nsQ = (u32)(d->n_start % Q);
-    u64 x = Q;
-    for (u64 f = 2; f * f <= x; ++f) {
-        if (x % f) continue;
-        d->qf_l[d->qf_n++] = (u32)f;
-        while (x % f == 0) x /= f;
-    }
-    if (x > 1) d->qf_l[d->qf_n++] = (u32)x;
+// The item's device constants with the default tuning: the split modulus
+// and the baby-step sizing of the regular entry points (fingerprint words, at
+// most one baby step per word on average, 2^11 words at most).
+int noalloc_item(const mps_item* it, DevItem* d, u32* tbits) {
+    const char* why = "";
+    if (int r = item_constants(it, 0, 0, d, &why)) return r;
     const u64 m_opt = (u64)std::ceil(std::sqrt((double)std::max<u64>(d->K, 1)));
     u32 tb = 6;
-    while ((1ull << tb) < 5 * m_opt && tb < 11) ++tb;
+    while ((1ull << (tb - 1)) < m_opt && tb < 11) ++tb;
     *tbits = tb;
-    d->max_baby = std::max<u32>((1u << tb) / 5, 1);
+    d->max_baby = std::min<u32>(1u << (tb - 1), kMaxBaby);
     return MPS_OK;
 }
 
@@ -180,8 +141,8 @@ u32 prime_count_below_sqrt(u64 hi) {
     return n;
 }
 
-// Host staging for one pass's raw relations (static storage, shared by calls).
-RawRelation g_host_rel[kNoAllocRelations];
+// Raw relations are read back through a small buffer on the caller's stack.
+constexpr u64 kReadBatch = 128;
 
 struct Sink {
     mps_relation* out;
@@ -196,7 +157,7 @@ int run_pass(unsigned char* base, u64 lo, u64 hi, const DevItem& d, u32 tbits, i
     Entry* ent = (Entry*)(base + kOffEnt);
     RawRelation* rel = (RawRelation*)(base + kOffRel);
     const SieveTables tables{(const u32*)(base + kOffSp), (const u64*)(base + kOffRcp), (const u64*)(base + kOffInv)};
-    const cudaStream_t s = 0;
+    const cudaStream_t s = cudaStreamPerThread;
 
     const u64 lo_odd = std::max<u64>(lo, 3) | 1ull;
     SieveArgs sa{};
@@ -217,6 +178,7 @@ int run_pass(unsigned char* base, u64 lo, u64 hi, const DevItem& d, u32 tbits, i
     pa.ent_cap = kNoAllocEntries;
     pa.rel = rel;
     pa.rel_cap = kNoAllocRelations;
+    pa.m_cap = std::min<u32>(1u << (tbits - 1), kMaxBaby);   // fingerprint words: 2^(tbits-1) keys
     BsgsArgs ba{};
     ba.ent = ent;
     ba.ent_cap = kNoAllocEntries;
@@ -226,6 +188,8 @@ int run_pass(unsigned char* base, u64 lo, u64 hi, const DevItem& d, u32 tbits, i
     ba.warps_per_block = 4;
     ba.persistent = 1;
     ba.chains = 2;
+    ba.table_kind = 0;
+    ba.load_shift = kDefaultLoadShift;
     ba.max_p = hi;
     OrderArgs oa{};
     oa.rel = rel;
@@ -253,16 +217,21 @@ int run_pass(unsigned char* base, u64 lo, u64 hi, const DevItem& d, u32 tbits, i
         return run_pass(base, mid, hi, d, tbits, num_sms, sink);
     }
     const u64 nr = h.relations;
-    if (nr && cudaMemcpy(g_host_rel, rel, nr * sizeof(RawRelation), cudaMemcpyDeviceToHost) != cudaSuccess)
-        return MPS_E_CUDA;
-    for (u64 i = 0; i < nr; ++i) {
-        if (g_host_rel[i].q == ~0ull) continue;
-        if (sink.n < sink.cap) {
-            sink.out[sink.n].p = g_host_rel[i].p;
-            sink.out[sink.n].M = g_host_rel[i].M;
-            sink.out[sink.n].q = g_host_rel[i].q;
+    RawRelation buf[kReadBatch];
+    for (u64 i0 = 0; i0 < nr; i0 += kReadBatch) {
+        const u64 k = std::min<u64>(kReadBatch, nr - i0);
+        if (cudaMemcpyAsync(buf, rel + i0, k * sizeof(RawRelation), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            return MPS_E_CUDA;
+        for (u64 i = 0; i < k; ++i) {
+            if (buf[i].q == ~0ull) continue;      // a composite survivor
+            if (sink.n < sink.cap) {
+                sink.out[sink.n].p = buf[i].p;
+                sink.out[sink.n].M = buf[i].M;
+                sink.out[sink.n].q = buf[i].q;
+            }
+            ++sink.n;
         }
-        ++sink.n;
     }
     return MPS_OK;
 }
@@ -277,7 +246,7 @@ extern "C" int mps_chunk_relations_noalloc(uint64_t lo, uint64_t hi, const mps_i
     if (hi > (1ull << 62) || hi - lo > kNoAllocMaxSpan) return MPS_E_RANGE;
     DevItem d;
     u32 tbits = 0;
-    if (int r = item_constants(item, &d, &tbits)) return r;
+    if (int r = noalloc_item(item, &d, &tbits)) return r;
     int code = MPS_OK;
     unsigned char* base = scratch_for_current_device(&code);
     if (!base) return code;

@@ -49,7 +49,7 @@ class Tuning(ctypes.Structure):
         ("bsgs_warps", ctypes.c_uint32), ("class_modulus", ctypes.c_uint32),
         ("full_mr", ctypes.c_uint32), ("plain", ctypes.c_uint32),
         ("chains", ctypes.c_uint32), ("graphs_off", ctypes.c_uint32), ("table_kind", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 4),
+        ("load_shift", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 3),
     ]
 
 
@@ -58,7 +58,8 @@ class Stats(ctypes.Structure):
         ("odds", ctypes.c_uint64), ("survivors", ctypes.c_uint64), ("entries", ctypes.c_uint64),
         ("relations", ctypes.c_uint64), ("chunks", ctypes.c_uint64), ("device_ms", ctypes.c_double),
         ("bsgs_ms", ctypes.c_double), ("bsgs_launches", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint64),
-        ("bsgs_steps", ctypes.c_uint64),
+        ("bsgs_steps", ctypes.c_uint64), ("sieve_ms", ctypes.c_double), ("prep_ms", ctypes.c_double),
+        ("order_ms", ctypes.c_double),
     ]
 
 
@@ -71,7 +72,15 @@ class ServeConfig(ctypes.Structure):
 class ServeStatus(ctypes.Structure):
     _fields_ = [("ticket", ctypes.c_uint64), ("state", ctypes.c_int32), ("error", ctypes.c_int32),
                 ("p_done", ctypes.c_uint64), ("relations", ctypes.c_uint64),
-                ("latency_ms", ctypes.c_double), ("queue_ms", ctypes.c_double)]
+                ("latency_ms", ctypes.c_double), ("queue_ms", ctypes.c_double),
+                ("reserved_bytes", ctypes.c_uint64), ("relations_on_device", ctypes.c_int32), ("pad", ctypes.c_int32)]
+
+
+class TuneReport(ctypes.Structure):
+    _fields_ = [("k_bits", ctypes.c_uint32), ("mod", ctypes.c_uint32), ("p_digits", ctypes.c_uint32),
+                ("candidates", ctypes.c_uint32), ("table_kind", ctypes.c_uint32), ("load_shift", ctypes.c_uint32),
+                ("chains", ctypes.c_uint32), ("warps", ctypes.c_uint32), ("best_ns_per_prime", ctypes.c_double),
+                ("default_ns_per_prime", ctypes.c_double), ("calib_bsgs_primes", ctypes.c_uint64)]
 
 
 def split128(v: int) -> tuple[int, int]:
@@ -124,7 +133,13 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.mps_serve_release.argtypes = [vp, u64]
     L.mps_serve_checkpoint.argtypes = [vp, u64, P(u64), P(u64)]
     L.mps_serve_close.argtypes = [vp]
+    L.mps_serve_pool.argtypes = [vp, P(u64), P(u64), P(u32), P(u32)]
     L.mps_measure_peaks.argtypes = [vp, P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_double)]
+    L.mps_measure_smem_peak.argtypes = [vp, P(ctypes.c_double)]
+    L.mps_autotune.argtypes = [vp, P(Item), sz, P(TuneReport), sz, P(sz)]
+    L.mps_tune_save.argtypes = [vp, ctypes.c_char_p]
+    L.mps_tune_load.argtypes = [vp, ctypes.c_char_p]
+    L.mps_tune_clear.argtypes = [vp]
     L.mps_test_survivors.argtypes = [vp, u64, u64, P(u64), sz, P(sz)]
     L.mps_test_is_prime.argtypes = [vp, P(u64), sz, P(ctypes.c_uint8)]
     L.mps_test_bsgs.argtypes = [vp, P(u64), sz, u32, P(u64)]
@@ -251,7 +266,28 @@ class Siever:
     def measure_peaks(self) -> dict:
         a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         self._check(self.lib.mps_measure_peaks(self.ctx, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
-        return {"fp64_mulmod_per_s": a.value, "int_mulmod_per_s": b.value, "imad_per_s": c.value}
+        d = ctypes.c_double()
+        self._check(self.lib.mps_measure_smem_peak(self.ctx, ctypes.byref(d)))
+        return {"fp64_mulmod_per_s": a.value, "int_mulmod_per_s": b.value, "imad_per_s": c.value,
+                "smem_atomic_per_s": d.value}
+
+    def autotune(self, items: list[Item]) -> list[dict]:
+        """Tunes the BSGS configuration of every item class among items (mps_autotune)."""
+        arr = (Item * max(len(items), 1))(*items)
+        n = ctypes.c_size_t()
+        cap = max(len(items), 1)
+        out = (TuneReport * cap)()
+        self._check(self.lib.mps_autotune(self.ctx, arr, len(items), out, cap, ctypes.byref(n)))
+        return [{k: getattr(out[i], k) for k, _ in TuneReport._fields_} for i in range(n.value)]
+
+    def tune_save(self, path: str):
+        self._check(self.lib.mps_tune_save(self.ctx, path.encode()))
+
+    def tune_load(self, path: str):
+        self._check(self.lib.mps_tune_load(self.ctx, path.encode()))
+
+    def tune_clear(self):
+        self._check(self.lib.mps_tune_clear(self.ctx))
 
     def survivors(self, lo: int, hi: int, cap: int = 1 << 16) -> list[int]:
         while True:
@@ -336,6 +372,14 @@ class Server:
         if rc != MPS_OK:
             raise MpsError(rc, "checkpoint")
         return a.value, b.value
+
+    def pool(self) -> dict:
+        a, b = ctypes.c_uint64(), ctypes.c_uint64()
+        c, d = ctypes.c_uint32(), ctypes.c_uint32()
+        rc = self.lib.mps_serve_pool(self.sv, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d))
+        if rc != MPS_OK:
+            raise MpsError(rc, "pool")
+        return {"pool_bytes": a.value, "reserved_bytes": b.value, "active": c.value, "queued": d.value}
 
     def close(self):
         if self.sv:

@@ -69,7 +69,7 @@ def _bsgs_cases(seed, count):
 
 
 @pytest.mark.parametrize("table_bits", [5, 6, 9, 12, 13])
-@pytest.mark.parametrize("table_kind", [0, 1])
+@pytest.mark.parametrize("table_kind", [0, 1, 2])
 def test_bsgs_smallest_j(mps_lib, oracle, table_bits, table_kind):
     cases = _bsgs_cases(100 + table_bits, 400)
     with mps_lib.Siever(0, table_kind=table_kind) as s:
@@ -125,6 +125,9 @@ def test_c1_prime_count(siever, golden):
     dict(class_modulus=2), dict(class_modulus=48), dict(class_modulus=720), dict(chunk_odds=40_000),
     dict(bsgs_warps=1), dict(bsgs_warps=8, table_bits=11), dict(table_kind=1), dict(table_kind=1, chains=4),
     dict(chains=1), dict(chains=4), dict(table_bits=7, max_baby=256), dict(graphs_off=1),
+    dict(table_kind=2), dict(table_kind=2, chains=1), dict(table_kind=2, chains=4), dict(table_kind=2, load_shift=3),
+    dict(table_kind=2, load_shift=1, table_bits=7), dict(table_kind=2, bsgs_warps=8), dict(class_modulus=1),
+    dict(class_modulus=1, plain=1),
 ])
 def test_tunings_give_identical_relations(mps_lib, oracle, tuning):
     specs = [(2, -25, 10**10, 10**10 + 4_000_000, 3_600_000, 5_000_000, 2, 1),

@@ -1,0 +1,49 @@
+"""The autotuner (mps_autotune): every candidate configuration gives the same
+relations (checked inside the tuner), the chosen one reproduces the
+reference-built golden relations, and the tuning cache round-trips."""
+from __future__ import annotations
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+NAMES = ("selftest", "c2_low", "c3_low", "b7_nomod", "b12_mod12", "mod48", "wide_n", "small_p_10", "b_128bit")
+
+
+def test_tuned_relations_equal_golden(mps_lib, golden, tmp_path):
+    cases = [c for c in golden["cases"] if c["name"] in NAMES]
+    items = [mps_lib.make_item(*c["item"]) for c in cases]
+    with mps_lib.Siever(0) as s:
+        reports = s.autotune(items)
+        assert reports and all(r["candidates"] >= 10 for r in reports)
+        for r in reports:
+            assert r["table_kind"] in (0, 2) and r["chains"] in (1, 2, 4) and r["warps"] in (4, 8)
+            assert r["best_ns_per_prime"] <= r["default_ns_per_prime"] * 1.0001
+        for c, it in zip(cases, items):
+            assert [list(x) for x in s.item_relations(it)] == c["relations"], c["name"]
+        got = s.batch_relations(items)
+        for k, c in enumerate(cases):
+            assert [[p, M, q] for i, p, M, q in got if i == k] == c["relations"], c["name"]
+        path = str(tmp_path / "tune.txt")
+        s.tune_save(path)
+    text = open(path).read().splitlines()
+    assert text[0] == "mps-tune 1" and len(text) == 1 + len(reports)
+    with mps_lib.Siever(0) as s2:
+        s2.tune_load(path)
+        for c, it in zip(cases, items):
+            assert [list(x) for x in s2.item_relations(it)] == c["relations"], c["name"]
+        s2.tune_clear()
+
+
+def test_tuning_file_with_bad_lines(mps_lib, tmp_path, golden):
+    path = tmp_path / "tune.txt"
+    # a kind, chain count and warp count the kernels are not built for are skipped
+    path.write_text("mps-tune 1\n1 9 2 2 4 1.0\n2 2 2 3 4 1.0\n3 2 2 2 99 1.0\n")
+    case = next(c for c in golden["cases"] if c["name"] == "selftest")
+    with mps_lib.Siever(0) as s:
+        s.tune_load(str(path))
+        assert [list(x) for x in s.item_relations(mps_lib.make_item(*case["item"]))] == case["relations"]
+    (tmp_path / "bad.txt").write_text("not a tuning file\n")
+    with mps_lib.Siever(0) as s:
+        with pytest.raises(mps_lib.MpsError):
+            s.tune_load(str(tmp_path / "bad.txt"))

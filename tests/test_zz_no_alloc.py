@@ -56,6 +56,22 @@ def test_matches_regular_entry_point_twice(siever, mps_lib):
             assert got == want, (b, c, lo, hi)
 
 
+def test_matches_golden_relations(mps_lib, golden):
+    """Slices of non-empty reference-built golden items, each no wider than
+    the entry point takes, against the golden relations of that slice."""
+    call = _noalloc(mps_lib)
+    for name in ("c2_low", "c3_low", "small_p_2", "selftest"):
+        case = next(c for c in golden["cases"] if c["name"] == name)
+        b, c, P0, P1, N0, N1, mod, res = case["item"]
+        hi = min(P1, P0 + SPAN_LIMIT)
+        want = [tuple(r) for r in case["relations"] if r[0] < hi]
+        item = mps_lib.make_item(b, c, P0, hi, N0, N1, mod, res)
+        for _ in range(2):
+            rc, got, n = call(P0, hi, item)
+            assert rc == mps_lib.MPS_OK and n == len(want)
+            assert got == want, name
+
+
 def test_rejects_ranges_beyond_its_scratch(mps_lib):
     call = _noalloc(mps_lib)
     item = mps_lib.make_item(2, -25, 10**9, 10**9 + SPAN_LIMIT + 2, 0, 1000, 1, 0)
