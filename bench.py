@@ -460,6 +460,60 @@ def served(local: int, duration: float, max_width: int) -> dict:
             "rates": results, "best_primes_per_s": max(r["primes_per_s"] for r in results), "clocks": clk}
 
 
+def reference_gpu(local: int, width: int) -> dict:
+    """The reference's own GPU worker path on the same GPU: its kernels (psieve,
+    prep_sv/prep_svq, bsgs_wg/bsgs_wq, collect, compiled ahead of time from its
+    Gpu.hpp by baseline/ref_gpu) driven chunk by chunk as its
+    CudaSiever::sieve_filter does, with the flagged numbers checked exactly on
+    all host threads (is_prime64 + run_bsgs) while the GPU sieves the next
+    chunk.  On [P0, P0 + width) of the default item; relations compared with
+    the reference-built fixture."""
+    import ctypes
+    import gzip
+    path = os.path.join(ROOT, "baseline", "_ref", "ref_gpu", "librefgpu.so")
+    if not os.path.exists(path):
+        return {"unavailable": "baseline/_ref/ref_gpu/librefgpu.so is not built (needs the reference tree)"}
+    import mps_b200
+
+    class Item(ctypes.Structure):
+        _fields_ = mps_b200.Item._fields_
+
+    class Rel(ctypes.Structure):
+        _fields_ = [("p", ctypes.c_uint64), ("M", ctypes.c_uint64), ("q", ctypes.c_uint64)]
+
+    class Stats(ctypes.Structure):
+        _fields_ = [("seconds", ctypes.c_double), ("gpu_ms", ctypes.c_double), ("flagged", ctypes.c_uint64),
+                    ("declined", ctypes.c_uint64)]
+
+    L = ctypes.CDLL(path)
+    L.refgpu_relations.argtypes = [ctypes.c_int, ctypes.POINTER(Item), ctypes.c_uint64, ctypes.c_int,
+                                   ctypes.POINTER(Rel), ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t),
+                                   ctypes.POINTER(Stats)]
+    b, c, P0, _, N0, N1, mod, res, _ = WORKLOADS["c2"]
+    it = mps_b200.make_item(b, c, P0, P0 + width, N0, N1, mod, res)
+    item = Item(*[getattr(it, f) for f, _ in Item._fields_])
+    threads = os.cpu_count() or 1
+    chunk = 1 << 28
+    cap = 1 << 16
+    out = (Rel * cap)()
+    n = ctypes.c_size_t()
+    st = Stats()
+    for _ in range(2):                                     # the second run is kept (the first sets up)
+        rc = L.refgpu_relations(local, ctypes.byref(item), chunk, threads, out, cap, ctypes.byref(n), ctypes.byref(st))
+        if rc != 0:
+            return {"unavailable": f"refgpu_relations returned {rc}"}
+    rels = [(out[i].p, out[i].M, out[i].q) for i in range(n.value)]
+    with gzip.open(os.path.join(ROOT, "tests", "golden", "c2_full.txt.gz"), "rt") as f:
+        want = [tuple(int(x) for x in line.split(",")) for line in f if int(line.split(",")[0]) < P0 + width]
+    with mps_b200.Siever(local) as s:
+        nprimes = s.count_primes(P0, P0 + width)
+    return {"value": nprimes / st.seconds, "unit": "primes/s", "sample": f"[1e12, 1e12+{width:.3g}) of the default item",
+            "seconds": st.seconds, "gpu_ms": st.gpu_ms, "cpu_threads": threads, "chunk": chunk,
+            "flagged": st.flagged, "declined_chunks": st.declined, "relations": len(rels),
+            "parity": "ok" if rels == want else "mismatch",
+            "path": "reference kernels (Gpu.hpp) via a restated CudaSiever::sieve_filter, exact CPU check of flagged"}
+
+
 # -------------------------------------------------------------------- main --
 
 def headline(args, rank, world, local, dist) -> dict:
@@ -548,20 +602,24 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + ["c4", "c5"])
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + ["c4", "c5", "refgpu"])
     ap.add_argument("--duration", type=float, default=10.0, help="served: seconds of arrivals per rate")
     ap.add_argument("--serve-width", type=float, default=1e9, help="served: P width cap per item")
     ap.add_argument("--width", type=float, default=None, help="P width per rank (default: the workload's)")
     ap.add_argument("--plain", action="store_true", help="the plain per-chunk path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-sub", action="store_true", help="skip the batched and served sub-records")
+    ap.add_argument("--no-sub", action="store_true", help="skip the batched, served and reference-GPU sub-records")
     args = ap.parse_args()
 
     if args.impl == "reference":
-        spec = WORKLOADS["c2" if args.workload in ("c4", "c5") else args.workload]
+        spec = WORKLOADS["c2" if args.workload in ("c4", "c5", "refgpu") else args.workload]
         return run_reference(args, spec, spec[-1])
 
     rank, world, local, dist = dist_setup(args.gpus)
+    if args.workload == "refgpu":
+        if rank == 0:
+            print(json.dumps(reference_gpu(local, int(args.width) if args.width else 10**9)), flush=True)
+        return 0
     if args.workload in ("c4", "c5"):
         if rank == 0:
             if args.workload == "c4":
@@ -578,6 +636,7 @@ def main():
     if world == 1 and args.workload == "c2" and args.width is None and not args.no_sub:
         line["batched_vs_plain"] = batched_vs_plain(local, 1, 1)
         line["served"] = served(local, args.duration, int(args.serve_width))
+        line["reference_gpu"] = reference_gpu(local, 10**9)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
