@@ -196,9 +196,11 @@ int mps_serve_close(mps_server* sv);
  * For every item class among items -- the bit length of K (the item's count of
  * in-class exponents), the class modulus, the decimal digits of P0 -- times
  * each candidate BSGS configuration (table kind, table load, chains per lane,
- * warps per block) with CUDA events on a calibration slice of the item (its
- * first 2^25 integers), checks that every candidate gives the same relations,
- * and keeps the fastest for the class.  Later calls on items of a tuned class
+ * warps per block) by the BSGS kernel's CUDA events on a calibration slice of
+ * the item (its first 2^25 integers), then with the fastest the sieve's
+ * segment size (1024, 2048 or 4096 words) by the sieve kernel's events;
+ * checks that every candidate gives the same relations, and keeps the
+ * fastest configuration for the class.  Later calls on items of a tuned class
  * use it (per item; a batched wave uses the configuration of its item with
  * the largest K).  One report per class tuned; MPS_E_CAPACITY if cap is too
  * small (*n_out = the number of classes).  The tuning changes speed only:
@@ -208,14 +210,18 @@ typedef struct mps_tune_report {
     uint32_t mod;                 /* class: class modulus (capped at 4095)               */
     uint32_t p_digits;            /* class: decimal digits of P0, minus one              */
     uint32_t candidates;          /* configurations timed                                */
-    uint32_t table_kind, load_shift, chains, warps;   /* the configuration chosen        */
+    uint32_t table_kind, load_shift, chains, warps;   /* the BSGS configuration chosen   */
+    uint32_t seg_words;           /* the sieve segment chosen (words of 32 odd numbers)  */
+    uint32_t pad;
     double   best_ns_per_prime;   /* BSGS time per prime reaching the BSGS, chosen       */
     double   default_ns_per_prime;/* the same under the context's tuning fields          */
+    double   sieve_best_ms;       /* sieve time of the calibration slice, chosen segment */
+    double   sieve_default_ms;    /* the same with the default segment (2048 words)      */
     uint64_t calib_bsgs_primes;   /* primes of the calibration slice reaching the BSGS   */
 } mps_tune_report;
 int mps_autotune(mps_ctx* ctx, const mps_item* items, size_t n_items, mps_tune_report* out, size_t cap,
                  size_t* n_out);
-/* The tuned classes as text ("mps-tune 1" then one line per class); mps_open
+/* The tuned classes as text ("mps-tune 2" then one line per class); mps_open
  * loads the file named by the environment variable MPS_TUNE_CACHE, if set. */
 int mps_tune_save(const mps_ctx* ctx, const char* path);
 int mps_tune_load(mps_ctx* ctx, const char* path);

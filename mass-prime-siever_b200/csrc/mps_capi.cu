@@ -57,19 +57,21 @@ const HostTables& host_tables() {
 
 }  // namespace
 
-// One BSGS launch configuration (what the autotuner chooses per item class):
-// the table kind, its load (table kind 2), chains per lane and warps per block.
-struct BsgsCfg {
-    u32 kind = 0, load_shift = kDefaultLoadShift, chains = 2, warps = 4;
-    bool operator==(const BsgsCfg& o) const {
-        return kind == o.kind && load_shift == o.load_shift && chains == o.chains && warps == o.warps;
+// One launch configuration (what the autotuner chooses per item class): the
+// BSGS table kind, its load (table kind 2), chains per lane and warps per
+// block, and the sieve's segment size.
+struct LaunchCfg {
+    u32 kind = 0, load_shift = kDefaultLoadShift, chains = 2, warps = 4, seg_words = kDefaultSegWords;
+    bool operator==(const LaunchCfg& o) const {
+        return kind == o.kind && load_shift == o.load_shift && chains == o.chains && warps == o.warps &&
+               seg_words == o.seg_words;
     }
-    bool operator!=(const BsgsCfg& o) const { return !(*this == o); }
+    bool operator!=(const LaunchCfg& o) const { return !(*this == o); }
 };
 
 // A tuned configuration with the calibration that chose it.
 struct TuneEntry {
-    BsgsCfg cfg;
+    LaunchCfg cfg;
     double ns_per_prime = 0;       // BSGS device time per prime of the calibration slice
 };
 
@@ -97,7 +99,7 @@ struct WaveSlot {
     struct Graph {
         cudaGraphExec_t exec = nullptr;
         u32 tbits = 0;
-        BsgsCfg cfg;
+        LaunchCfg cfg;
     };
     std::vector<Graph> graphs;
     const DevItem* graph_items = nullptr;     // the buffers the graphs were captured with
@@ -138,7 +140,7 @@ struct mps_ctx {
     WaveSlot slot[2];
     bool slots_ready = false;
     std::vector<u64> item_K;           // K of each item on the device (table sizing)
-    std::vector<BsgsCfg> item_cfg;     // BSGS configuration of each item on the device
+    std::vector<LaunchCfg> item_cfg;     // BSGS configuration of each item on the device
     std::map<u64, TuneEntry> tuned;    // autotuned configurations by item class (tune_key)
     std::vector<RawRelation> last;     // relations of the last call (kept for mps_take_relations)
 
@@ -203,8 +205,8 @@ int ensure_rel(mps_ctx* c, u64 need) {
 u32 load_shift_of(const mps_ctx* c) { return c->tun.load_shift ? std::min<u32>(c->tun.load_shift, 4) : kDefaultLoadShift; }
 
 // The configuration the tuning fields ask for.
-BsgsCfg default_cfg(const mps_ctx* c) {
-    BsgsCfg g;
+LaunchCfg default_cfg(const mps_ctx* c) {
+    LaunchCfg g;
     g.kind = c->tun.table_kind;
     g.load_shift = load_shift_of(c);
     g.chains = c->tun.chains ? c->tun.chains : 2;
@@ -225,13 +227,13 @@ u64 tune_key(u64 K, u64 cm, u64 P0) {
 }
 
 // The configuration for an item: the tuned one of its class, else the default.
-BsgsCfg cfg_for(const mps_ctx* c, u64 K, u64 cm, u64 P0) {
+LaunchCfg cfg_for(const mps_ctx* c, u64 K, u64 cm, u64 P0) {
     auto it = c->tuned.find(tune_key(K, cm, P0));
     return it != c->tuned.end() ? it->second.cfg : default_cfg(c);
 }
 
 // Keys a table of 4 << tb bytes holds under configuration g.
-u32 table_holds(const BsgsCfg& g, u32 tb) {
+u32 table_holds(const LaunchCfg& g, u32 tb) {
     if (g.kind == 0) return 1u << (tb - 1);
     if (g.kind == 2) return 1u << (tb + 1 - g.load_shift);
     return std::max<u32>((1u << tb) / 5, 1);
@@ -246,7 +248,7 @@ u32 table_holds(const BsgsCfg& g, u32 tb) {
 // 2^tbits slots, load at most 1/5 (a probe then reads one slot).  16-bit
 // slots (table_kind 2): 2^(tbits+1) slots, a prime's keys at most
 // 2^-load_shift of them (up to 12 bits, 16 KB per warp, when load_shift > 2).
-void table_for(const mps_ctx* c, const BsgsCfg& g, u64 K, u32* tbits, u32* max_baby) {
+void table_for(const mps_ctx* c, const LaunchCfg& g, u64 K, u32* tbits, u32* max_baby) {
     const u64 m_opt = (u64)std::ceil(std::sqrt((double)std::max<u64>(K, 1)));
     const u32 top = g.kind == 2 && g.load_shift > 2 ? 12 : 11;
     u32 tb = c->tun.table_bits;
@@ -265,7 +267,7 @@ void table_for(const mps_ctx* c, const BsgsCfg& g, u64 K, u32* tbits, u32* max_b
 
 // The baby-step cap of a launch with configuration g and tables of 4 << tbits
 // bytes: no prime of the launch gets more, whatever its item's own sizing.
-u32 launch_m_cap(const mps_ctx* c, const BsgsCfg& g, u32 tbits) {
+u32 launch_m_cap(const mps_ctx* c, const LaunchCfg& g, u32 tbits) {
     const u32 cap = g.kind == 0 ? (1u << tbits) : g.kind == 2 ? (1u << tbits) : (1u << tbits) - 1;
     const u32 holds = c->tun.max_baby ? std::max(c->tun.max_baby, table_holds(g, tbits)) : table_holds(g, tbits);
     return std::max<u32>(1, std::min<u32>(std::min<u32>(holds, cap), kMaxBaby));
@@ -274,10 +276,10 @@ u32 launch_m_cap(const mps_ctx* c, const BsgsCfg& g, u32 tbits) {
 // The device constants of an item (mps_item.cuh), with this context's split
 // modulus, the item's BSGS configuration (tuned or default) and its
 // baby-step sizing.
-int make_dev_item(mps_ctx* c, const mps_item* it, u32 index, DevItem* d, BsgsCfg* cfg = nullptr) {
+int make_dev_item(mps_ctx* c, const mps_item* it, u32 index, DevItem* d, LaunchCfg* cfg = nullptr) {
     const char* why = "";
     if (int r = item_constants(it, c->tun.class_modulus, index, d, &why)) return fail(c, r, why);
-    const BsgsCfg g = cfg_for(c, d->K, d->cm, it->P0);
+    const LaunchCfg g = cfg_for(c, d->K, d->cm, it->P0);
     u32 tb = 0, mb = 0;
     table_for(c, g, d->K, &tb, &mb);
     d->max_baby = mb;
@@ -327,7 +329,7 @@ int bsgs_grid(mps_ctx* c, u32 tbits, u32 warps, int* grid) {
 
 // Relations of the primes of one device chunk [lo, hi) (at most chunk_odds
 // odd numbers) for item `item`, already on the device.  Appends RawRelations.
-int run_chunk(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, const BsgsCfg& g, std::vector<RawRelation>& out) {
+int run_chunk(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, const LaunchCfg& g, std::vector<RawRelation>& out) {
     const u64 lo_odd = std::max<u64>(lo, 3) | 1ull;
     const u64 n_odds = lo_odd < hi ? (hi - lo_odd + 1) / 2 : 0;
     const u32 include_two = (lo <= 2 && hi > 2) ? 1 : 0;
@@ -385,7 +387,7 @@ int run_chunk(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, const BsgsCfg& g, std
     cudaStream_t s = c->stream;
     CK(cudaMemsetAsync(c->d_ctr, 0, sizeof(Counters), s), "counter reset");
     CK(cudaEventRecord(c->evk[0], s), "event");
-    CK(launch_sieve(sa, c->tables(), c->d_surv, nullptr, c->surv_cap, c->d_ctr, s), "sieve launch");
+    CK(launch_sieve(sa, c->tables(), c->d_surv, nullptr, c->surv_cap, c->d_ctr, s, g.seg_words), "sieve launch");
     CK(cudaEventRecord(c->evk[1], s), "event");
     int bgrid = 0;
     if (int r = bsgs_grid(c, tbits, warps, &bgrid)) return r;
@@ -516,7 +518,7 @@ void slot_free(WaveSlot& w) {
 }
 
 // The per-wave launch sequence on the slot's stream (captured or direct).
-int slot_enqueue(mps_ctx* c, WaveSlot& w, u32 tbits, const BsgsCfg& g, bool capturing) {
+int slot_enqueue(mps_ctx* c, WaveSlot& w, u32 tbits, const LaunchCfg& g, bool capturing) {
     const cudaStream_t s = w.stream;
     const u32 warps = g.warps;
     PrepArgs pa{};
@@ -538,7 +540,8 @@ int slot_enqueue(mps_ctx* c, WaveSlot& w, u32 tbits, const BsgsCfg& g, bool capt
     // external records: a captured graph records these events on every replay
     const unsigned ev_flags = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
     CK(cudaEventRecordWithFlags(w.evk[0], s, ev_flags), "event");
-    CK(launch_sieve_wave(w.d_wave, c->tables(), w.d_surv, w.d_surv_item, w.surv_cap, w.d_ctr, grid_for(c, 8), s),
+    CK(launch_sieve_wave(w.d_wave, c->tables(), w.d_surv, w.d_surv_item, w.surv_cap, w.d_ctr, grid_for(c, 8), s,
+                         g.seg_words),
        "sieve launch");
     CK(cudaEventRecordWithFlags(w.evk[1], s, ev_flags), "event");
     CK(cudaEventRecordWithFlags(w.evk[2], s, ev_flags), "event");
@@ -557,7 +560,7 @@ int slot_enqueue(mps_ctx* c, WaveSlot& w, u32 tbits, const BsgsCfg& g, bool capt
     return MPS_OK;
 }
 
-int slot_launch(mps_ctx* c, WaveSlot& w, u32 tbits, const BsgsCfg& cfg) {
+int slot_launch(mps_ctx* c, WaveSlot& w, u32 tbits, const LaunchCfg& cfg) {
     if (c->tun.graphs_off) return slot_enqueue(c, w, tbits, cfg, false);
     if (w.graph_items != c->d_items || w.graph_state != c->d_state) {
         drop_graphs(w);
@@ -592,10 +595,20 @@ int slot_launch(mps_ctx* c, WaveSlot& w, u32 tbits, const BsgsCfg& cfg) {
     return MPS_OK;
 }
 
+// Numbers the segments of a wave's runs (segments of seg_words * 32 odd numbers).
+void set_segments(WaveDesc* wave, u32 seg_words) {
+    const u64 seg_odds = (u64)seg_words * 32;
+    wave->total_segs = 0;
+    for (u32 r = 0; r < wave->n_runs; ++r) {
+        wave->runs[r].seg_begin = wave->total_segs;
+        wave->total_segs += (wave->runs[r].n_odds + seg_odds - 1) / seg_odds;
+    }
+}
+
 // The launch shape of a wave: the configuration of its item with the most
 // in-class exponents (whose BSGS dominates the wave), with tables large
 // enough for every item in it.
-void wave_shape(const mps_ctx* c, const WaveSlot& w, u32* tbits, BsgsCfg* g) {
+void wave_shape(const mps_ctx* c, const WaveSlot& w, u32* tbits, LaunchCfg* g) {
     u32 top = w.range_item[0];
     for (u32 it : w.range_item)
         if (c->item_K[it] > c->item_K[top]) top = it;
@@ -669,14 +682,10 @@ int run_waves(mps_ctx* c, const std::vector<u64>& lo, const std::vector<u64>& hi
     u64 wave_odds = 0;
     auto flush = [&]() -> int {
         if (!cur || cur->h_wave->n_runs == 0) return MPS_OK;
-        cur->h_wave->total_segs = 0;
-        for (u32 r = 0; r < cur->h_wave->n_runs; ++r) {
-            cur->h_wave->runs[r].seg_begin = cur->h_wave->total_segs;
-            cur->h_wave->total_segs += (cur->h_wave->runs[r].n_odds + kSieveSegOdds - 1) / kSieveSegOdds;
-        }
         u32 tbits;
-        BsgsCfg g;
+        LaunchCfg g;
         wave_shape(c, *cur, &tbits, &g);
+        set_segments(cur->h_wave, g.seg_words);
         if (int r = slot_launch(c, *cur, tbits, g)) return r;
         cur->busy = true;
         k ^= 1;
@@ -919,7 +928,7 @@ void serve_loop(mps_server* sv) {
     const u64 chunk = c->tun.chunk_odds;
     // every wave of the server has one launch shape: the default configuration
     // with the tables of the widest N range (launch_m_cap keeps every prime within them)
-    const BsgsCfg cfg = default_cfg(c);
+    const LaunchCfg cfg = default_cfg(c);
     u32 tbits = 11;
     {
         u32 mb;
@@ -1034,11 +1043,7 @@ void serve_loop(mps_server* sv) {
                     if (q->cursor < q->item.P1) more = true;
                 }
             }
-            w.h_wave->total_segs = 0;
-            for (u32 r = 0; r < w.h_wave->n_runs; ++r) {
-                w.h_wave->runs[r].seg_begin = w.h_wave->total_segs;
-                w.h_wave->total_segs += (w.h_wave->runs[r].n_odds + kSieveSegOdds - 1) / kSieveSegOdds;
-            }
+            set_segments(w.h_wave, cfg.seg_words);
             const int r = slot_launch(c, w, tbits, cfg);
             if (r) {
                 serve_fail_all(sv, r, c->err);
@@ -1076,7 +1081,7 @@ int end_call(mps_ctx* c) {
 }
 
 // [lo, hi) in device chunks of at most chunk_odds odd numbers.
-int run_range(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, const BsgsCfg& g, std::vector<RawRelation>& rel) {
+int run_range(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, const LaunchCfg& g, std::vector<RawRelation>& rel) {
     const u64 chunk = c->tun.chunk_odds;
     for (u64 a = lo; a < hi;) {
         const u64 lo_odd = std::max<u64>(a, 3) | 1ull;
@@ -1090,7 +1095,7 @@ int run_range(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, const BsgsCfg& g, std
 
 int relations_of(mps_ctx* c, const mps_item* item, u64 lo, u64 hi, std::vector<RawRelation>& rel) {
     DevItem d;
-    BsgsCfg g;
+    LaunchCfg g;
     if (int r = make_dev_item(c, item, 0, &d, &g)) return r;
     if (lo >= hi) return MPS_OK;
     if (hi > kTwo62) return fail(c, MPS_E_RANGE, "hi must not exceed 2^62");
@@ -1230,7 +1235,7 @@ int mps_item_relations(mps_ctx* c, const mps_item* item, mps_relation* out, size
     if (c && c->tun.plain) return mps_chunk_relations(c, item->P0, item->P1, item, out, cap, n_out);
     if (int r = check_ctx(c)) return r;
     DevItem d;
-    BsgsCfg g;
+    LaunchCfg g;
     if (int r = make_dev_item(c, item, 0, &d, &g)) return r;
     begin_call(c);
     std::vector<RawRelation> rel;
@@ -1264,7 +1269,7 @@ int mps_filter(mps_ctx* c, const uint64_t* primes, size_t n, const mps_item* ite
     if (n == 0) return MPS_OK;
     if (!primes || !flags) return fail(c, MPS_E_ARG, "NULL buffer");
     DevItem d;
-    BsgsCfg g;
+    LaunchCfg g;
     if (int r = make_dev_item(c, item, 0, &d, &g)) return r;
     for (size_t i = 0; i < n; ++i)
         if (primes[i] >= kTwo62) return fail(c, MPS_E_RANGE, "primes must be below 2^62");
@@ -1330,7 +1335,7 @@ int mps_batch_relations(mps_ctx* c, const mps_item* items, size_t n_items, mps_r
     if (int r = check_ctx(c)) return r;
     if (!items && n_items) return fail(c, MPS_E_ARG, "items is NULL");
     std::vector<DevItem> d(n_items);
-    std::vector<BsgsCfg> cfg(n_items);
+    std::vector<LaunchCfg> cfg(n_items);
     for (size_t i = 0; i < n_items; ++i)
         if (int r = make_dev_item(c, &items[i], (u32)i, &d[i], &cfg[i])) return r;
     begin_call(c);
@@ -1618,14 +1623,14 @@ int mps_autotune(mps_ctx* c, const mps_item* items, size_t n_items, mps_tune_rep
     if (!items && n_items) return fail(c, MPS_E_ARG, "items is NULL");
     if (!out && cap) return fail(c, MPS_E_ARG, "out is NULL");
     constexpr u64 kCalibSpan = 1ull << 25;
-    const BsgsCfg base = default_cfg(c);
-    std::vector<BsgsCfg> cands{base};
+    const LaunchCfg base = default_cfg(c);
+    std::vector<LaunchCfg> cands{base};
     for (u32 kind : {0u, 2u})
         for (u32 ls : {2u, 3u}) {
             if (kind != 2 && ls != 2) continue;
             for (u32 ch : {1u, 2u, 4u})
                 for (u32 w : {4u, 8u}) {
-                    BsgsCfg g;
+                    LaunchCfg g;
                     g.kind = kind;
                     g.load_shift = kind == 2 ? ls : base.load_shift;
                     g.chains = ch;
@@ -1642,23 +1647,39 @@ int mps_autotune(mps_ctx* c, const mps_item* items, size_t n_items, mps_tune_rep
         const u64 key = tune_key(d.K, d.cm, items[i].P0);
         if (!seen.insert(key).second || !d.has_work) continue;
         const u64 lo = items[i].P0, hi = std::min<u64>(items[i].P1, items[i].P0 + kCalibSpan);
-        double best_ms = 0, base_ms = 0;
+        double best_ms = 0, base_ms = 0, sieve_base_ms = 0, sieve_best_ms = 0;
         u64 entries = 0;
-        BsgsCfg best = base;
+        LaunchCfg best = base;
         std::vector<RawRelation> first;
+        // phase 1: the BSGS configuration by the BSGS kernel's time; phase 2: with
+        // it, the sieve's segment size by the sieve kernel's time
+        std::vector<LaunchCfg> segs;
+        for (u32 w : {1024u, 2048u, 4096u}) {
+            LaunchCfg g = base;
+            g.seg_words = w;
+            segs.push_back(g);
+        }
+        const size_t n_bsgs = cands.size();
+        cands.insert(cands.end(), segs.begin(), segs.end());
         for (size_t k = 0; k < cands.size(); ++k) {
-            const BsgsCfg& g = cands[k];
+            LaunchCfg g = cands[k];
+            if (k >= n_bsgs) {                                  // phase 2 keeps the chosen BSGS settings
+                const u32 w = g.seg_words;
+                g = best;
+                g.seg_words = w;
+            }
             u32 tb, mb;
             table_for(c, g, d.K, &tb, &mb);
             d.max_baby = mb;
             if (bsgs_smem_bytes(tb, g.warps) > c->smem_optin) continue;
             if (int r = upload_items(c, &d, 1)) return r;
-            double ms = 0;
+            double ms = 0, sms = 0;
             for (int rep = 0; rep < 2; ++rep) {                 // the second run is timed
                 std::vector<RawRelation> rel;
                 std::memset(&c->stats, 0, sizeof(c->stats));
                 if (int r = run_chunk(c, lo, hi, 0, d.K, g, rel)) return r;
                 ms = c->stats.bsgs_ms;
+                sms = c->stats.sieve_ms;
                 entries = c->stats.entries;
                 sort_by_p(rel);
                 if (k == 0 && rep == 0) {
@@ -1670,12 +1691,21 @@ int mps_autotune(mps_ctx* c, const mps_item* items, size_t n_items, mps_tune_rep
                     return fail(c, MPS_E_CUDA, "tuning candidates gave different relations");
                 }
             }
-            if (k == 0) base_ms = ms;
-            if (k == 0 || ms < best_ms) {
-                best_ms = ms;
-                best = g;
+            if (k < n_bsgs) {
+                if (k == 0) base_ms = ms;
+                if (k == 0 || ms < best_ms) {
+                    best_ms = ms;
+                    best = g;
+                }
+            } else {
+                if (g.seg_words == base.seg_words) sieve_base_ms = sms;
+                if (k == n_bsgs || sms < sieve_best_ms) {
+                    sieve_best_ms = sms;
+                    best.seg_words = g.seg_words;
+                }
             }
         }
+        cands.resize(n_bsgs);
         const double per = entries ? 1e6 / (double)entries : 0.0;
         TuneEntry te;
         te.cfg = best;
@@ -1690,6 +1720,9 @@ int mps_autotune(mps_ctx* c, const mps_item* items, size_t n_items, mps_tune_rep
         rp.load_shift = best.load_shift;
         rp.chains = best.chains;
         rp.warps = best.warps;
+        rp.seg_words = best.seg_words;
+        rp.sieve_best_ms = sieve_best_ms;
+        rp.sieve_default_ms = sieve_base_ms;
         rp.best_ns_per_prime = best_ms * per;
         rp.default_ns_per_prime = base_ms * per;
         rp.calib_bsgs_primes = entries;
@@ -1706,10 +1739,11 @@ int mps_tune_save(const mps_ctx* c, const char* path) {
     if (!c || !path) return MPS_E_ARG;
     FILE* f = std::fopen(path, "w");
     if (!f) return MPS_E_ARG;
-    std::fprintf(f, "mps-tune 1\n");
+    std::fprintf(f, "mps-tune 2\n");
     for (const auto& kv : c->tuned)
-        std::fprintf(f, "%llu %u %u %u %u %.3f\n", (unsigned long long)kv.first, kv.second.cfg.kind,
-                     kv.second.cfg.load_shift, kv.second.cfg.chains, kv.second.cfg.warps, kv.second.ns_per_prime);
+        std::fprintf(f, "%llu %u %u %u %u %u %.3f\n", (unsigned long long)kv.first, kv.second.cfg.kind,
+                     kv.second.cfg.load_shift, kv.second.cfg.chains, kv.second.cfg.warps, kv.second.cfg.seg_words,
+                     kv.second.ns_per_prime);
     return std::fclose(f) == 0 ? MPS_OK : MPS_E_ARG;
 }
 
@@ -1718,21 +1752,24 @@ int mps_tune_load(mps_ctx* c, const char* path) {
     FILE* f = std::fopen(path, "r");
     if (!f) return fail(c, MPS_E_ARG, std::string("cannot open ") + path);
     char head[32] = {0};
-    if (!std::fgets(head, sizeof(head), f) || std::strncmp(head, "mps-tune 1", 10) != 0) {
+    if (!std::fgets(head, sizeof(head), f) || std::strncmp(head, "mps-tune 2", 10) != 0) {
         std::fclose(f);
         return fail(c, MPS_E_ARG, "not a tuning file");
     }
     unsigned long long key;
-    unsigned kind, ls, ch, w;
+    unsigned kind, ls, ch, w, sw;
     double ns;
-    while (std::fscanf(f, "%llu %u %u %u %u %lf", &key, &kind, &ls, &ch, &w, &ns) == 6) {
+    while (std::fscanf(f, "%llu %u %u %u %u %u %lf", &key, &kind, &ls, &ch, &w, &sw, &ns) == 7) {
         // only configurations the kernels are built for
-        if (kind > 2 || ls < 1 || ls > 4 || (ch != 1 && ch != 2 && ch != 4) || w < 1 || w > 8) continue;
+        if (kind > 2 || ls < 1 || ls > 4 || (ch != 1 && ch != 2 && ch != 4) || w < 1 || w > 8 ||
+            (sw != 1024 && sw != 2048 && sw != 4096))
+            continue;
         TuneEntry te;
         te.cfg.kind = kind;
         te.cfg.load_shift = ls;
         te.cfg.chains = ch;
         te.cfg.warps = w;
+        te.cfg.seg_words = sw;
         te.ns_per_prime = ns;
         c->tuned[key] = te;
     }

@@ -71,10 +71,11 @@ __device__ __forceinline__ void emit_relation(u64 p, u64 M, u64 q, u32 item, Raw
 
 // -------------------------------------------------------------- the sieve --
 
-constexpr u32 kSegWords = 2048;               // 8 KB bitmap
-constexpr u32 kSegOdds = kSegWords * 32;      // 65,536 odd numbers per segment
+// A segment is W words of shared-memory bitmap (W * 32 odd numbers); W is a
+// template parameter (1024, 2048 or 4096 words: 4, 8 or 16 KB), chosen per
+// launch.  kSegWords is the default.
+constexpr u32 kSegWords = 2048;
 constexpr u32 kSieveThreads = 256;
-constexpr u32 kWordsPerThread = kSegWords / kSieveThreads;
 constexpr u32 kNumPattern = 10;               // 3..31: whole-word patterns, no atomics
 constexpr u32 kNumMedium = 171;               // primes below 1024: all threads share each prime
 
@@ -95,8 +96,9 @@ __device__ __forceinline__ u64 first_strike(u64 v0, u32 q, u64 rcp) {
     return j;
 }
 
+template <u32 W>
 struct SieveShared {
-    u32 bits[kSegWords];
+    u32 bits[W];
     u32 med_start[kNumMedium];
     u32 warp_sum[kSieveThreads / 32];
     unsigned long long block_base;
@@ -112,11 +114,13 @@ __device__ __forceinline__ void emit_two(u32 item, u64* surv, u32* surv_item, u6
     }
 }
 
-// One segment of len <= kSegOdds odd numbers v0, v0 + 2, ... (v0 odd, >= 3),
+// One segment of len <= W * 32 odd numbers v0, v0 + 2, ... (v0 odd, >= 3),
 // sieved by the first n_primes odd primes; survivors appended to surv[].
 // Called by all threads of the block.
-__device__ void sieve_segment(SieveShared& sh, u64 v0, u32 len, u32 n_primes, u32 item, const SieveTables& t,
+template <u32 W>
+__device__ void sieve_segment(SieveShared<W>& sh, u64 v0, u32 len, u32 n_primes, u32 item, const SieveTables& t,
                               u64* surv, u32* surv_item, u64 cap, Counters* ctr) {
+    constexpr u32 kSegOdds = W * 32, kWordsPerThread = W / kSieveThreads;
     const u32 tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const u32 n_med = min(n_primes, kNumMedium);
     // 1. primes 3..31: each thread writes whole words (pattern << offset).
@@ -135,7 +139,7 @@ __device__ void sieve_segment(SieveShared& sh, u64 v0, u32 len, u32 n_primes, u3
             off[k] = (u32)o;
             step[k] = (32u * kSieveThreads) % q;
         }
-        for (u32 w = tid; w < kSegWords; w += kSieveThreads) {
+        for (u32 w = tid; w < W; w += kSieveThreads) {
             u32 word = 0;
 #pragma unroll
             for (u32 k = 0; k < kNumPattern; ++k) {
@@ -225,9 +229,11 @@ __device__ void sieve_segment(SieveShared& sh, u64 v0, u32 len, u32 n_primes, u3
     __syncthreads();
 }
 
+template <u32 W>
 __global__ void __launch_bounds__(kSieveThreads) k_sieve(SieveArgs a, SieveTables t, u64* surv, u32* surv_item,
                                                          u64 cap, Counters* ctr) {
-    __shared__ SieveShared sh;
+    constexpr u32 kSegOdds = W * 32;
+    __shared__ SieveShared<W> sh;
     if (blockIdx.x == 0 && threadIdx.x == 0 && a.include_two) emit_two(a.item, surv, surv_item, cap, ctr);
     for (u64 seg = blockIdx.x; seg * kSegOdds < a.n_odds; seg += gridDim.x) {
         const u64 base = seg * kSegOdds;
@@ -238,9 +244,11 @@ __global__ void __launch_bounds__(kSieveThreads) k_sieve(SieveArgs a, SieveTable
 
 // The same over a wave of runs (ranges of possibly different items), read
 // from device memory so that a captured graph can be replayed per wave.
+template <u32 W>
 __global__ void __launch_bounds__(kSieveThreads) k_sieve_wave(const WaveDesc* w, SieveTables t, u64* surv,
                                                               u32* surv_item, u64 cap, Counters* ctr) {
-    __shared__ SieveShared sh;
+    constexpr u32 kSegOdds = W * 32;
+    __shared__ SieveShared<W> sh;
     const u32 n_runs = w->n_runs;
     const u64 total = w->total_segs;
     if (blockIdx.x == 0 && threadIdx.x == 0)
@@ -1792,18 +1800,27 @@ __global__ void k_order_direct(const u64* bp, u64* q_out, u64 count, SieveTables
 
 size_t bsgs_smem_bytes(u32 tbits, u32 warps_per_block) { return (size_t)warps_per_block * (4u << tbits); }
 
+bool valid_seg_words(u32 seg_words) { return seg_words == 1024 || seg_words == 2048 || seg_words == 4096; }
+
 cudaError_t launch_sieve(const SieveArgs& a, const SieveTables& t, u64* surv, u32* surv_item, u64 surv_cap,
-                         Counters* ctr, cudaStream_t s) {
-    const u64 segs = (a.n_odds + kSegOdds - 1) / kSegOdds;
+                         Counters* ctr, cudaStream_t s, u32 seg_words) {
+    if (!valid_seg_words(seg_words)) return cudaErrorInvalidValue;
+    const u64 seg_odds = (u64)seg_words * 32;
+    const u64 segs = (a.n_odds + seg_odds - 1) / seg_odds;
     if (segs == 0 && !a.include_two) return cudaSuccess;
     const u64 grid = segs == 0 ? 1 : min(segs, (u64)148 * 8);
-    k_sieve<<<(unsigned)grid, kSieveThreads, 0, s>>>(a, t, surv, surv_item, surv_cap, ctr);
+    if (seg_words == 1024) k_sieve<1024><<<(unsigned)grid, kSieveThreads, 0, s>>>(a, t, surv, surv_item, surv_cap, ctr);
+    else if (seg_words == 4096) k_sieve<4096><<<(unsigned)grid, kSieveThreads, 0, s>>>(a, t, surv, surv_item, surv_cap, ctr);
+    else k_sieve<2048><<<(unsigned)grid, kSieveThreads, 0, s>>>(a, t, surv, surv_item, surv_cap, ctr);
     return cudaGetLastError();
 }
 
 cudaError_t launch_sieve_wave(const WaveDesc* w, const SieveTables& t, u64* surv, u32* surv_item, u64 surv_cap,
-                              Counters* ctr, int grid, cudaStream_t s) {
-    k_sieve_wave<<<grid, kSieveThreads, 0, s>>>(w, t, surv, surv_item, surv_cap, ctr);
+                              Counters* ctr, int grid, cudaStream_t s, u32 seg_words) {
+    if (!valid_seg_words(seg_words)) return cudaErrorInvalidValue;
+    if (seg_words == 1024) k_sieve_wave<1024><<<grid, kSieveThreads, 0, s>>>(w, t, surv, surv_item, surv_cap, ctr);
+    else if (seg_words == 4096) k_sieve_wave<4096><<<grid, kSieveThreads, 0, s>>>(w, t, surv, surv_item, surv_cap, ctr);
+    else k_sieve_wave<2048><<<grid, kSieveThreads, 0, s>>>(w, t, surv, surv_item, surv_cap, ctr);
     return cudaGetLastError();
 }
 

@@ -24,8 +24,10 @@ struct SieveArgs {
     u32 item;          // item index stored with the survivors
 };
 
+// seg_words: segment bitmap words (1024, 2048 or 4096; 32 odd numbers each)
+constexpr u32 kDefaultSegWords = 2048;
 cudaError_t launch_sieve(const SieveArgs& a, const SieveTables& t, u64* surv, u32* surv_item, u64 surv_cap,
-                         Counters* ctr, cudaStream_t s);
+                         Counters* ctr, cudaStream_t s, u32 seg_words = kDefaultSegWords);
 
 // A wave: several runs (odd ranges of possibly different items) sieved by
 // one launch; kept in device memory so that a captured graph is replayable.
@@ -59,15 +61,15 @@ struct WaveDesc {
     u64 total_segs;
     SieveRun runs[kMaxRuns];
 };
-constexpr u64 kSieveSegOdds = 65536;   // odd numbers per sieve segment (one block)
 // After a wave: advance each run's item to the run's end, count relations.
 cudaError_t launch_commit(const WaveDesc* w, const RawRelation* rel, const Counters* ctr, u64 rel_cap,
                           ItemState* st, cudaStream_t s);
 // A run of an overflowed wave, redone on the host path: p_done = max(p_done, hi),
 // its n relations rel[0..n) appended to the item's state.
 cudaError_t launch_state_add(ItemState* st, u32 item, u64 hi, const RawRelation* rel, u64 n, cudaStream_t s);
+// The wave's runs' seg_begin must count segments of seg_words * 32 odd numbers.
 cudaError_t launch_sieve_wave(const WaveDesc* w, const SieveTables& t, u64* surv, u32* surv_item, u64 surv_cap,
-                              Counters* ctr, int grid, cudaStream_t s);
+                              Counters* ctr, int grid, cudaStream_t s, u32 seg_words = kDefaultSegWords);
 
 // Prep: filters, primality screen and BSGS set-up for every survivor.
 struct PrepArgs {
