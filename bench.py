@@ -330,18 +330,43 @@ def profile_traffic(kernel: str):
 
 # ------------------------------------------------------------- sub-records --
 
-def batched_vs_plain(local: int, steps: int, warmup: int, max_width=None) -> dict:
+def tuning_summary(reports: list[dict], seconds: float) -> dict:
+    """The autotuner's choices: how many item classes chose each configuration."""
+    counts: dict[str, int] = {}
+    for r in reports:
+        key = (f"kind{r['table_kind']}" + (f"/load2^-{r['load_shift']}" if r["table_kind"] == 2 else "") +
+               f"/ch{r['chains']}/w{r['warps']}/seg{r['seg_words']}")
+        counts[key] = counts.get(key, 0) + 1
+    gain = [r["default_ns_per_prime"] / r["best_ns_per_prime"] for r in reports if r["best_ns_per_prime"] > 0]
+    return {"classes": len(reports), "seconds": seconds, "choices": counts,
+            "bsgs_gain_vs_default": {"min": min(gain), "median": statistics.median(gain), "max": max(gain)}
+            if gain else None}
+
+
+def batched_vs_plain(local: int, steps: int, warmup: int, max_width=None, tune: bool = True) -> dict:
     """The 64-item mixed batch (C4): batched engine vs the plain per-item GPU path
     (each item alone, plain-method filter Q = lcm(mod, 2), stage-by-stage
     launches with a host read of each stage's count, one BSGS warp per prime)
     vs each item alone through the default engine.  Same chunk size (2^26 odd
     numbers) and table defaults everywhere.  Relations must agree exactly."""
     import mps_b200
+    import tempfile
     import workloads
     specs = workloads.c4_items(max_width=max_width)
     items = [mps_b200.make_item(*sp) for sp in specs]
+    tune_file = os.path.join(tempfile.mkdtemp(prefix="mps_tune_"), "tune.txt")
     with mps_b200.Siever(local) as s:
         nprimes = sum(s.count_primes(sp[2], sp[3]) for sp in specs)
+        # one tuning for every path compared (outside every timed region)
+        t0 = time.perf_counter()
+        reports = s.autotune(items) if tune else []
+        tune_s = time.perf_counter() - t0
+        s.tune_save(tune_file)
+
+    def open_siever(**kw):
+        sv = mps_b200.Siever(local, **kw)
+        sv.tune_load(tune_file)
+        return sv
 
     def batched(s):
         t0 = time.perf_counter()
@@ -363,7 +388,7 @@ def batched_vs_plain(local: int, steps: int, warmup: int, max_width=None) -> dic
         return out, dev, wall, launches
 
     clocks = ClockSampler(local).start()
-    with mps_b200.Siever(local) as s:
+    with open_siever() as s:
         for _ in range(warmup):
             batched(s)
         dev_b, wall_b, l_b = 0.0, 0.0, 0
@@ -371,11 +396,11 @@ def batched_vs_plain(local: int, steps: int, warmup: int, max_width=None) -> dic
             rel_b, d, w, l = batched(s)
             dev_b, wall_b, l_b = dev_b + d, wall_b + w, l_b + l
     short = mps_b200.make_item(*specs[0][:3], specs[0][2] + 10**8, *specs[0][4:])
-    with mps_b200.Siever(local, plain=1, class_modulus=1) as s:
+    with open_siever(plain=1, class_modulus=1) as s:
         for _ in range(warmup):
             s.item_relations(short)
         rel_p, dev_p, wall_p, l_p = per_item(s)
-    with mps_b200.Siever(local) as s:
+    with open_siever() as s:
         for _ in range(warmup):
             s.item_relations(short)
         rel_a, dev_a, wall_a, l_a = per_item(s)
@@ -411,6 +436,7 @@ def batched_vs_plain(local: int, steps: int, warmup: int, max_width=None) -> dic
         "ratio_vs_plain": b_rate / (nprimes / dev_p),
         "ratio_vs_alone": b_rate / (nprimes / dev_a),
         "parity": parity, "golden_first_1e8": golden, "clocks": clk,
+        "tuning": tuning_summary(reports, tune_s),
     }
     return rec
 
@@ -530,6 +556,10 @@ def headline(args, rank, world, local, dist) -> dict:
     # units: primes in this rank's slice (counted on the device, outside the timed region)
     nprimes = siever.count_primes(lo, hi)
     total_primes = reduce_over_ranks(dist, local, float(nprimes), "sum")
+    # the autotuner's choice for this item (outside the timed region)
+    t0 = time.perf_counter()
+    reports = siever.autotune([item]) if not args.no_tune else []
+    tuning = tuning_summary(reports, time.perf_counter() - t0)
 
     for _ in range(args.warmup):
         siever.item_relations(item)
@@ -591,7 +621,7 @@ def headline(args, rank, world, local, dist) -> dict:
         "gpu_launches": acc["kernel_launches"], "relations": len(rels), "parity": parity,
         "bsgs_primes": entries, "primes": int(total_primes),
         "stage_ms_per_step": {k: acc[k] / steps for k in ("sieve_ms", "prep_ms", "bsgs_ms", "order_ms")},
-        "roofline": roof, "kernels": kernels, "single_stream_shares": shares,
+        "roofline": roof, "kernels": kernels, "single_stream_shares": shares, "tuning": tuning,
         "cpu_baseline": cpu, "clocks": clk,
     }
 
@@ -608,6 +638,7 @@ def main():
     ap.add_argument("--width", type=float, default=None, help="P width per rank (default: the workload's)")
     ap.add_argument("--plain", action="store_true", help="the plain per-chunk path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="run the default configuration instead of the tuned one")
     ap.add_argument("--no-sub", action="store_true", help="skip the batched, served and reference-GPU sub-records")
     args = ap.parse_args()
 
@@ -624,7 +655,7 @@ def main():
         if rank == 0:
             if args.workload == "c4":
                 rec = batched_vs_plain(local, args.steps, min(args.warmup, 1),
-                                       int(args.width) if args.width else None)
+                                       int(args.width) if args.width else None, tune=not args.no_tune)
             else:
                 rec = served(local, args.duration, int(args.serve_width))
             print(json.dumps(rec), flush=True)
@@ -634,7 +665,7 @@ def main():
 
     line = headline(args, rank, world, local, dist)
     if world == 1 and args.workload == "c2" and args.width is None and not args.no_sub:
-        line["batched_vs_plain"] = batched_vs_plain(local, 1, 1)
+        line["batched_vs_plain"] = batched_vs_plain(local, 1, 1, tune=not args.no_tune)
         line["served"] = served(local, args.duration, int(args.serve_width))
         line["reference_gpu"] = reference_gpu(local, 10**9)
     if rank == 0:

@@ -191,7 +191,7 @@ struct Fp64 {
     __device__ __forceinline__ void init(u64 modulus) {
         pi = modulus;
         p = (double)modulus;
-        pinv = __ddiv_rn(1.0, p);
+        pinv = __drcp_rn(p);                   // correctly rounded 1/p (the value 1.0 / p gives)
     }
     __device__ __forceinline__ double mul(double a, double b) const {
         const double C = 6755399441055744.0;   // 1.5 * 2^52
