@@ -77,7 +77,9 @@ typedef struct mps_tuning {
                                    per slot, read with one 16-bit load per probe               */
     uint32_t load_shift;        /* table kind 2: a prime's table is at least 2^load_shift times
                                    its baby-step count (0: 2)                                  */
-    uint32_t reserved[3];
+    uint32_t lanes;             /* table kind 2: lanes per prime, 32, 16 or 8 (0: 32); groups of
+                                   16 or 8 solve 2 or 4 primes per warp, for p < 2^49          */
+    uint32_t reserved[2];
 } mps_tuning;
 
 /* Counters of the last call (all chunks of it). */
@@ -195,8 +197,8 @@ int mps_serve_close(mps_server* sv);
  * item, Cuda.hpp:342-348, and picks m and Gc per prime, Gpu.hpp:553-573) ----
  * For every item class among items -- the bit length of K (the item's count of
  * in-class exponents), the class modulus, the decimal digits of P0 -- times
- * each candidate BSGS configuration (table kind, table load, chains per lane,
- * warps per block) by the BSGS kernel's CUDA events on a calibration slice of
+ * each candidate BSGS configuration (table kind, table load, lanes per prime,
+ * chains per lane, warps per block) by the BSGS kernel's CUDA events on a calibration slice of
  * the item (its first 2^25 integers), then with the fastest the sieve's
  * segment size (1024, 2048 or 4096 words) by the sieve kernel's events;
  * checks that every candidate gives the same relations, and keeps the
@@ -212,7 +214,7 @@ typedef struct mps_tune_report {
     uint32_t candidates;          /* configurations timed                                */
     uint32_t table_kind, load_shift, chains, warps;   /* the BSGS configuration chosen   */
     uint32_t seg_words;           /* the sieve segment chosen (words of 32 odd numbers)  */
-    uint32_t pad;
+    uint32_t lanes;               /* lanes per prime chosen (32, or groups of 16 or 8)   */
     double   best_ns_per_prime;   /* BSGS time per prime reaching the BSGS, chosen       */
     double   default_ns_per_prime;/* the same under the context's tuning fields          */
     double   sieve_best_ms;       /* sieve time of the calibration slice, chosen segment */
@@ -221,7 +223,7 @@ typedef struct mps_tune_report {
 } mps_tune_report;
 int mps_autotune(mps_ctx* ctx, const mps_item* items, size_t n_items, mps_tune_report* out, size_t cap,
                  size_t* n_out);
-/* The tuned classes as text ("mps-tune 2" then one line per class); mps_open
+/* The tuned classes as text ("mps-tune 3" then one line per class); mps_open
  * loads the file named by the environment variable MPS_TUNE_CACHE, if set. */
 int mps_tune_save(const mps_ctx* ctx, const char* path);
 int mps_tune_load(mps_ctx* ctx, const char* path);

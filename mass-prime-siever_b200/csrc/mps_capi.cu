@@ -58,13 +58,14 @@ const HostTables& host_tables() {
 }  // namespace
 
 // One launch configuration (what the autotuner chooses per item class): the
-// BSGS table kind, its load (table kind 2), chains per lane and warps per
-// block, and the sieve's segment size.
+// BSGS table kind, its load (table kind 2), lanes per prime, chains per lane
+// and warps per block, and the sieve's segment size.
 struct LaunchCfg {
     u32 kind = 0, load_shift = kDefaultLoadShift, chains = 2, warps = 4, seg_words = kDefaultSegWords;
+    u32 lanes = 32;     // lanes per prime (table kind 2: 32, or groups of 16 / 8 for p < 2^49)
     bool operator==(const LaunchCfg& o) const {
         return kind == o.kind && load_shift == o.load_shift && chains == o.chains && warps == o.warps &&
-               seg_words == o.seg_words;
+               seg_words == o.seg_words && lanes == o.lanes;
     }
     bool operator!=(const LaunchCfg& o) const { return !(*this == o); }
 };
@@ -211,6 +212,9 @@ LaunchCfg default_cfg(const mps_ctx* c) {
     g.load_shift = load_shift_of(c);
     g.chains = c->tun.chains ? c->tun.chains : 2;
     g.warps = c->tun.bsgs_warps ? c->tun.bsgs_warps : 4;
+    const u32 lanes = c->tun.lanes;
+    // groups of lanes exist for the 16-bit slot table with 1 or 2 chains
+    g.lanes = g.kind == 2 && g.chains <= 2 && (lanes == 8 || lanes == 16) ? lanes : 32;
     return g;
 }
 
@@ -232,11 +236,22 @@ LaunchCfg cfg_for(const mps_ctx* c, u64 K, u64 cm, u64 P0) {
     return it != c->tuned.end() ? it->second.cfg : default_cfg(c);
 }
 
-// Keys a table of 4 << tb bytes holds under configuration g.
+// log2 of the primes a warp solves at once (lanes per prime 32, 16 or 8).
+u32 groups_log(const LaunchCfg& g) { return g.kind == 2 ? (g.lanes == 8 ? 2 : g.lanes == 16 ? 1 : 0) : 0; }
+
+// Keys a prime's table holds under configuration g with 4 << tb bytes per warp.
 u32 table_holds(const LaunchCfg& g, u32 tb) {
     if (g.kind == 0) return 1u << (tb - 1);
-    if (g.kind == 2) return 1u << (tb + 1 - g.load_shift);
+    if (g.kind == 2) return std::max<u32>(1u << (tb + 1 - g.load_shift) >> groups_log(g), 1);
     return std::max<u32>((1u << tb) / 5, 1);
+}
+
+// Room for a prime's keys (load at most 1/2 in 16-bit slots): fingerprint
+// words hold four keys each, 32-bit slots one.
+u32 table_room(const LaunchCfg& g, u32 tb) {
+    if (g.kind == 0) return 1u << tb;
+    if (g.kind == 2) return (1u << tb) >> groups_log(g);
+    return (1u << tb) - 1;
 }
 
 // Baby-step table size for an item: 4 << tbits bytes per warp, at most
@@ -258,9 +273,7 @@ void table_for(const mps_ctx* c, const LaunchCfg& g, u64 K, u32* tbits, u32* max
     }
     tb = std::min<u32>(std::max<u32>(tb, 6), 14);
     u32 mb = c->tun.max_baby ? c->tun.max_baby : table_holds(g, tb);
-    // room for the keys: fingerprint words hold four, 32-bit slots one, 16-bit slots one with load <= 1/2
-    const u32 cap = g.kind == 0 ? (1u << tb) : g.kind == 2 ? (1u << tb) : (1u << tb) - 1;
-    mb = std::min<u32>(std::min<u32>(mb, kMaxBaby), cap);
+    mb = std::min<u32>(std::min<u32>(mb, kMaxBaby), table_room(g, tb));
     *tbits = tb;
     *max_baby = std::max<u32>(mb, 1);
 }
@@ -268,9 +281,15 @@ void table_for(const mps_ctx* c, const LaunchCfg& g, u64 K, u32* tbits, u32* max
 // The baby-step cap of a launch with configuration g and tables of 4 << tbits
 // bytes: no prime of the launch gets more, whatever its item's own sizing.
 u32 launch_m_cap(const mps_ctx* c, const LaunchCfg& g, u32 tbits) {
-    const u32 cap = g.kind == 0 ? (1u << tbits) : g.kind == 2 ? (1u << tbits) : (1u << tbits) - 1;
     const u32 holds = c->tun.max_baby ? std::max(c->tun.max_baby, table_holds(g, tbits)) : table_holds(g, tbits);
-    return std::max<u32>(1, std::min<u32>(std::min<u32>(holds, cap), kMaxBaby));
+    return std::max<u32>(1, std::min<u32>(std::min<u32>(holds, table_room(g, tbits)), kMaxBaby));
+}
+
+// Groups of lanes per prime run the FP64 solve only: a range that reaches
+// 2^49 runs a whole warp per prime.
+LaunchCfg for_range(LaunchCfg g, u64 hi) {
+    if (hi > kFp64Limit) g.lanes = 32;
+    return g;
 }
 
 // The device constants of an item (mps_item.cuh), with this context's split
@@ -329,7 +348,8 @@ int bsgs_grid(mps_ctx* c, u32 tbits, u32 warps, int* grid) {
 
 // Relations of the primes of one device chunk [lo, hi) (at most chunk_odds
 // odd numbers) for item `item`, already on the device.  Appends RawRelations.
-int run_chunk(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, const LaunchCfg& g, std::vector<RawRelation>& out) {
+int run_chunk(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, const LaunchCfg& g_item, std::vector<RawRelation>& out) {
+    const LaunchCfg g = for_range(g_item, hi);
     const u64 lo_odd = std::max<u64>(lo, 3) | 1ull;
     const u64 n_odds = lo_odd < hi ? (hi - lo_odd + 1) / 2 : 0;
     const u32 include_two = (lo <= 2 && hi > 2) ? 1 : 0;
@@ -376,6 +396,7 @@ int run_chunk(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, const LaunchCfg& g, s
     ba.chains = g.chains;
     ba.table_kind = g.kind;
     ba.load_shift = g.load_shift;
+    ba.lanes = g.lanes;
     ba.max_p = hi;
 
     OrderArgs oa{};
@@ -435,6 +456,7 @@ int run_chunk(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, const LaunchCfg& g, s
         return run_chunk(c, lo, hi, item, K, g, out);
     }
     if (h.status & kStatusOrderFailed) return fail(c, MPS_E_CUDA, "order computation did not factor p - 1");
+    if (h.status & kStatusBadLaunch) return fail(c, MPS_E_CUDA, "a BSGS entry did not fit the launch's tables");
     const u64 nr = h.relations;
     if (nr) {
         CK(cudaMemcpyAsync(c->h_rel, c->d_rel, nr * sizeof(RawRelation), cudaMemcpyDeviceToHost, s), "relation read");
@@ -529,7 +551,7 @@ int slot_enqueue(mps_ctx* c, WaveSlot& w, u32 tbits, const LaunchCfg& g, bool ca
     BsgsArgs ba{};
     ba.ent = w.d_ent; ba.ent_cap = w.ent_cap; ba.rel = w.d_rel; ba.rel_cap = w.rel_cap; ba.tbits = tbits;
     ba.warps_per_block = warps; ba.persistent = 1; ba.chains = g.chains;
-    ba.table_kind = g.kind; ba.load_shift = g.load_shift;
+    ba.table_kind = g.kind; ba.load_shift = g.load_shift; ba.lanes = g.lanes;
     ba.max_p = 0;   // per-entry arithmetic
     OrderArgs oa{};
     oa.rel = w.d_rel; oa.rel_cap = w.rel_cap; oa.items = c->d_items; oa.tables = c->tables();
@@ -610,9 +632,11 @@ void set_segments(WaveDesc* wave, u32 seg_words) {
 // enough for every item in it.
 void wave_shape(const mps_ctx* c, const WaveSlot& w, u32* tbits, LaunchCfg* g) {
     u32 top = w.range_item[0];
+    u64 hi = 0;
     for (u32 it : w.range_item)
         if (c->item_K[it] > c->item_K[top]) top = it;
-    *g = c->item_cfg[top];
+    for (const auto& r : w.ranges) hi = std::max(hi, r.second);
+    *g = for_range(c->item_cfg[top], hi);
     *tbits = 6;
     for (u32 it : w.range_item) {
         u32 tb, mb;
@@ -631,6 +655,7 @@ int slot_finish(mps_ctx* c, WaveSlot& w, std::vector<RawRelation>& out) {
     if (int r = add_stage_times(c, w.evk)) return r;
     c->stats.kernel_launches += 5;
     if (h.status & kStatusOrderFailed) return fail(c, MPS_E_CUDA, "order computation did not factor p - 1");
+    if (h.status & kStatusBadLaunch) return fail(c, MPS_E_CUDA, "a BSGS entry did not fit the launch's tables");
     if (h.status & (kStatusSurvivorOverflow | kStatusEntryOverflow | kStatusRelationOverflow)) {
         // the commit kernel skipped this wave: redo its runs on the chunk path
         // (which splits or grows as needed) and record each in the item table
@@ -1301,6 +1326,7 @@ int mps_filter(mps_ctx* c, const uint64_t* primes, size_t n, const mps_item* ite
         ba.ent = c->d_ent; ba.ent_cap = c->ent_cap; ba.rel = c->d_rel; ba.rel_cap = c->rel_cap;
         ba.tbits = tbits; ba.warps_per_block = warps; ba.persistent = 1; ba.chains = g.chains; ba.table_kind = g.kind;
         ba.load_shift = g.load_shift;
+        ba.lanes = for_range(g, *std::max_element(primes + off, primes + off + cnt) + 1).lanes;
         ba.max_p = *std::max_element(primes + off, primes + off + cnt);
         OrderArgs oa{};
         oa.rel = c->d_rel; oa.rel_cap = c->rel_cap; oa.items = c->d_items; oa.tables = c->tables();
@@ -1309,7 +1335,7 @@ int mps_filter(mps_ctx* c, const uint64_t* primes, size_t n, const mps_item* ite
         CK(launch_order(oa, c->d_ctr, grid_for(c, 4), s), "order launch");
         CK(cudaMemcpyAsync(c->h_ctr, c->d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, s), "count read");
         CK(cudaStreamSynchronize(s), "filter");
-        if (c->h_ctr->status & (kStatusEntryOverflow | kStatusRelationOverflow | kStatusOrderFailed))
+        if (c->h_ctr->status & (kStatusEntryOverflow | kStatusRelationOverflow | kStatusOrderFailed | kStatusBadLaunch))
             return fail(c, MPS_E_CUDA, "filter buffers overflowed");
         const u64 nr = c->h_ctr->relations;
         if (nr) {
@@ -1638,6 +1664,18 @@ int mps_autotune(mps_ctx* c, const mps_item* items, size_t n_items, mps_tune_rep
                     if (g != base) cands.push_back(g);
                 }
         }
+    // lanes per prime: groups of 16 or 8 lanes (table kind 2, 1 or 2 chains)
+    for (u32 lanes : {16u, 8u})
+        for (u32 ch : {1u, 2u})
+            for (u32 w : {4u, 8u}) {
+                LaunchCfg g;
+                g.kind = 2;
+                g.load_shift = 2;
+                g.chains = ch;
+                g.warps = w;
+                g.lanes = lanes;
+                cands.push_back(g);
+            }
     std::vector<mps_tune_report> reps;
     std::set<u64> seen;
     for (size_t i = 0; i < n_items; ++i) {
@@ -1668,6 +1706,7 @@ int mps_autotune(mps_ctx* c, const mps_item* items, size_t n_items, mps_tune_rep
                 g = best;
                 g.seg_words = w;
             }
+            if (g.lanes != 32 && hi > kFp64Limit) continue;    // groups run the FP64 solve only
             u32 tb, mb;
             table_for(c, g, d.K, &tb, &mb);
             d.max_baby = mb;
@@ -1721,6 +1760,7 @@ int mps_autotune(mps_ctx* c, const mps_item* items, size_t n_items, mps_tune_rep
         rp.chains = best.chains;
         rp.warps = best.warps;
         rp.seg_words = best.seg_words;
+        rp.lanes = best.lanes;
         rp.sieve_best_ms = sieve_best_ms;
         rp.sieve_default_ms = sieve_base_ms;
         rp.best_ns_per_prime = best_ms * per;
@@ -1739,11 +1779,11 @@ int mps_tune_save(const mps_ctx* c, const char* path) {
     if (!c || !path) return MPS_E_ARG;
     FILE* f = std::fopen(path, "w");
     if (!f) return MPS_E_ARG;
-    std::fprintf(f, "mps-tune 2\n");
+    std::fprintf(f, "mps-tune 3\n");
     for (const auto& kv : c->tuned)
-        std::fprintf(f, "%llu %u %u %u %u %u %.3f\n", (unsigned long long)kv.first, kv.second.cfg.kind,
+        std::fprintf(f, "%llu %u %u %u %u %u %u %.3f\n", (unsigned long long)kv.first, kv.second.cfg.kind,
                      kv.second.cfg.load_shift, kv.second.cfg.chains, kv.second.cfg.warps, kv.second.cfg.seg_words,
-                     kv.second.ns_per_prime);
+                     kv.second.cfg.lanes, kv.second.ns_per_prime);
     return std::fclose(f) == 0 ? MPS_OK : MPS_E_ARG;
 }
 
@@ -1752,17 +1792,18 @@ int mps_tune_load(mps_ctx* c, const char* path) {
     FILE* f = std::fopen(path, "r");
     if (!f) return fail(c, MPS_E_ARG, std::string("cannot open ") + path);
     char head[32] = {0};
-    if (!std::fgets(head, sizeof(head), f) || std::strncmp(head, "mps-tune 2", 10) != 0) {
+    if (!std::fgets(head, sizeof(head), f) || std::strncmp(head, "mps-tune 3", 10) != 0) {
         std::fclose(f);
         return fail(c, MPS_E_ARG, "not a tuning file");
     }
     unsigned long long key;
-    unsigned kind, ls, ch, w, sw;
+    unsigned kind, ls, ch, w, sw, lanes;
     double ns;
-    while (std::fscanf(f, "%llu %u %u %u %u %u %lf", &key, &kind, &ls, &ch, &w, &sw, &ns) == 7) {
+    while (std::fscanf(f, "%llu %u %u %u %u %u %u %lf", &key, &kind, &ls, &ch, &w, &sw, &lanes, &ns) == 8) {
         // only configurations the kernels are built for
         if (kind > 2 || ls < 1 || ls > 4 || (ch != 1 && ch != 2 && ch != 4) || w < 1 || w > 8 ||
-            (sw != 1024 && sw != 2048 && sw != 4096))
+            (sw != 1024 && sw != 2048 && sw != 4096) || (lanes != 32 && lanes != 16 && lanes != 8) ||
+            (lanes != 32 && (kind != 2 || ch == 4)))
             continue;
         TuneEntry te;
         te.cfg.kind = kind;
@@ -1770,6 +1811,7 @@ int mps_tune_load(mps_ctx* c, const char* path) {
         te.cfg.chains = ch;
         te.cfg.warps = w;
         te.cfg.seg_words = sw;
+        te.cfg.lanes = lanes;
         te.ns_per_prime = ns;
         c->tuned[key] = te;
     }

@@ -19,6 +19,10 @@ typedef unsigned int u32;
 constexpr u32 kSievePrimes = 6541;
 constexpr u32 kSieveMaxPrime = 65521;
 
+// Moduli below this run the FP64-pipe arithmetic (exact for p < 2^49); larger
+// ones 64-bit Montgomery.
+constexpr u64 kFp64Limit = 1ull << 49;
+
 // Largest baby-step count of one prime (a table of 2^13 slots at load 1/2).
 constexpr u32 kMaxBaby = 4096;
 
@@ -88,5 +92,6 @@ constexpr u64 kStatusSurvivorOverflow = 1ull << 0;
 constexpr u64 kStatusEntryOverflow    = 1ull << 1;
 constexpr u64 kStatusRelationOverflow = 1ull << 2;
 constexpr u64 kStatusOrderFailed      = 1ull << 3;
+constexpr u64 kStatusBadLaunch        = 1ull << 4;   // an entry the launch's kernel cannot take (host sizing error)
 
 }  // namespace mps

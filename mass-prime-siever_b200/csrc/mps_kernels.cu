@@ -274,7 +274,6 @@ __global__ void __launch_bounds__(kSieveThreads) k_sieve_wave(const WaveDesc* w,
 // Two exact arithmetics behind one interface: FP64 (p < 2^49, the FP64 pipe)
 // and 64-bit Montgomery (p < 2^62, the integer pipe).  V is the value type;
 // key() gives the canonical integer (the table key) of a canonical value.
-constexpr u64 kFp64Limit = 1ull << 49;
 
 struct FieldF {
     typedef double V;
@@ -1393,6 +1392,16 @@ __device__ __forceinline__ u64 solve_any(const Entry& e, void* tab, u32 tbits, u
     return solve_fp64<CH ? CH : 1>(e, (u32*)tab, tbits, steps);
 }
 
+// Whether a prime's baby steps fit the table its solve will use (at most half
+// of its keys' room), so that every insertion finds a free slot.
+template <int CH, int QT>
+__device__ __forceinline__ bool fits_table(const Entry& e, u32 tbits) {
+    if (CH == 0 || e.p >= kFp64Limit) return e.m <= (1u << tbits);          // 2^(tbits+1) 16-bit slots
+    if (QT == 0) return e.m <= (1u << tbits);                               // 2^(tbits-1) words of four
+    if (QT == 2) return e.m <= (1u << tbits);                               // 2^(tbits+1) 16-bit slots
+    return e.m < (1u << tbits);                                            // 2^tbits 32-bit slots
+}
+
 // CH > 0: every entry has p < 2^49 (FP64 solve with CH chains per lane);
 // CH == 0: any p (integer Montgomery solve).
 template <int CH, int QT>
@@ -1409,6 +1418,10 @@ __global__ void __launch_bounds__(256, MPS_BSGS_MINB) k_bsgs(BsgsArgs a, Counter
             idx = __shfl_sync(FULL, idx, 0);
             if (idx >= n_ent) break;
             const Entry e = a.ent[idx];
+            if (!fits_table<CH, QT>(e, a.tbits)) {              // host sizing error: never overfill a table
+                if (lane == 0) atomicOr(&ctr->status, kStatusBadLaunch);
+                continue;
+            }
             u64 steps = 0;
             const u64 j = solve_any<CH, QT>(e, tab, a.tbits, a.load_shift, &steps);
             if (lane == 0) {
@@ -1421,6 +1434,10 @@ __global__ void __launch_bounds__(256, MPS_BSGS_MINB) k_bsgs(BsgsArgs a, Counter
         const u64 idx = (u64)blockIdx.x * a.warps_per_block + warp;
         if (idx >= n_ent) return;
         const Entry e = a.ent[idx];
+        if (!fits_table<CH, QT>(e, a.tbits)) {
+            if (lane == 0) atomicOr(&ctr->status, kStatusBadLaunch);
+            return;
+        }
         u64 steps = 0;
         const u64 j = solve_any<CH, QT>(e, tab, a.tbits, a.load_shift, &steps);
         if (lane == 0) {
@@ -1428,6 +1445,191 @@ __global__ void __launch_bounds__(256, MPS_BSGS_MINB) k_bsgs(BsgsArgs a, Counter
             atomicAdd(&ctr->steps, (unsigned long long)steps);
         }
     }
+}
+
+// ---- lanes per prime: L-lane groups, 32/L primes per warp in lockstep ----
+//
+// For primes with few baby and giant steps a whole warp per prime spends
+// most of its time on per-prime set-up (the lane-power scan, the table
+// clear).  Here a warp takes 32/L entries at once and each group of L lanes
+// solves one with its own 16-bit slot table (a 1/(32/L) share of the warp's
+// table memory); the loops run to the largest bound among the warp's primes
+// with per-group predicates, so the groups never diverge.  Same tables, same
+// exact resolution and the same smallest-j result as solve_fp64h.
+
+// Smallest i in [lo, limit) with t * B^i == v within the group (-1: none).
+// Warp-uniform control flow: a group with want == false only keeps pace.
+template <int L>
+__device__ int gfind_baby(const Fp64& f, double tbl, double BL, u32 lo, u32 limit, double v, bool want, u32 gl,
+                          u32 gshift, u32 gbits) {
+    const u32 lim_max = __reduce_max_sync(FULL, want ? limit : 0u);
+    double x = tbl;
+    int res = -1;
+    for (u32 base = 0; base < lim_max; base += L) {
+        const u32 i = base + gl;
+        const bool hit = want && res < 0 && i >= lo && i < limit && f.canon(x) == v;
+        const u32 gb = (__ballot_sync(FULL, hit) >> gshift) & gbits;
+        if (gb && res < 0) res = (int)(base + __ffs(gb) - 1);
+        if (__all_sync(FULL, !want || res >= 0 || base + L >= limit)) break;
+        x = f.mul(x, BL);
+    }
+    return res;
+}
+
+template <int L, int CH>
+__global__ void __launch_bounds__(256, MPS_BSGS_MINB) k_bsgs_groups(BsgsArgs a, Counters* ctr) {
+    constexpr u32 NG = 32 / L;
+    constexpr u32 NG_LOG = NG == 4 ? 2 : NG == 2 ? 1 : 0;
+    extern __shared__ __align__(16) u32 smem32[];
+    const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const u32 grp = lane / L, gl = lane % L, gshift = grp * L;
+    const u32 gbits = L == 32 ? FULL : (1u << L) - 1u;
+    const u32 group_slots = (2u << a.tbits) >> NG_LOG;          // 16-bit slots per group
+    unsigned short* tab = reinterpret_cast<unsigned short*>(smem32 + (size_t)warp * (1u << a.tbits)) +
+                          (size_t)grp * group_slots;
+    const u32 tw_max = a.tbits + 1 - NG_LOG;
+    const u64 n_ent = min((u64)*(volatile unsigned long long*)&ctr->entries, a.ent_cap);
+    u64 my_steps = 0;
+    for (;;) {
+        u64 first = 0;
+        if (lane == 0) first = atomicAdd(&ctr->work_next, (unsigned long long)NG);
+        first = __shfl_sync(FULL, first, 0);
+        if (first >= n_ent) break;
+        const u64 idx = first + grp;
+        Entry e = a.ent[idx < n_ent ? idx : n_ent - 1];
+        bool active = idx < n_ent;
+        // the host sends only p < 2^49 and at most half a group table of baby steps here
+        if (active && (e.p >= kFp64Limit || e.m > (1u << (tw_max - 1)))) {
+            if (gl == 0) atomicOr(&ctr->status, kStatusBadLaunch);
+            active = false;
+        }
+        Fp64 f;
+        f.init(active ? e.p : 1000003ull);
+        const u32 m = active ? e.m : 0;
+        const u32 jc = active ? (u32)e.jcount : 0;
+        const u32 tw = min(tw_max, max(6u, 32u - __clz(max(m, 2u) - 1) + a.load_shift));
+        const u32 mask = (1u << tw) - 1, shift = 32 - tw;
+        const double B = active ? (double)e.B : 1.0, Bm = active ? (double)e.Bm : 1.0;
+        const double tv = active ? (double)e.t : 1.0, G0 = active ? (double)e.G0 : 1.0;
+
+        double xb = B, xg = Bm;                                 // B^(gl+1), Bm^(gl+1)
+#pragma unroll
+        for (int off = 1; off < L; off <<= 1) {
+            const double yb = __shfl_up_sync(FULL, xb, off, L), yg = __shfl_up_sync(FULL, xg, off, L);
+            if (gl >= (u32)off) {
+                xb = f.mul(xb, yb);
+                xg = f.mul(xg, yg);
+            }
+        }
+        const double BL = __shfl_sync(FULL, xb, L - 1, L), BmL = __shfl_sync(FULL, xg, L - 1, L);
+        double bl = __shfl_up_sync(FULL, xb, 1, L);
+        if (gl == 0) bl = 1.0;
+        double Bstep = BL, Gstep = BmL;                         // B^(L CH), Bm^(L CH)
+#pragma unroll
+        for (int c = 1; c < CH; c <<= 1) {
+            Bstep = f.mul(Bstep, Bstep);
+            Gstep = f.mul(Gstep, Gstep);
+        }
+        const double tbl = f.mul(tv, bl);
+        double bx[CH], gx[CH];
+        bx[0] = tbl;
+        gx[0] = f.mul(G0, xg);
+#pragma unroll
+        for (int c = 1; c < CH; ++c) {
+            bx[c] = f.mul(bx[c - 1], BL);
+            gx[c] = f.mul(gx[c - 1], BmL);
+        }
+        uint4* t4 = reinterpret_cast<uint4*>(tab);
+        for (u32 k = gl; k <= (mask >> 3); k += L) t4[k] = make_uint4(0, 0, 0, 0);
+        __syncwarp();
+
+        // baby steps, each group stopping at its own cycle B^d == 1 (d < m)
+        u32 cyc = 0, baby_done = m;
+        bool bdone = m == 0;
+        const u32 m_max = __reduce_max_sync(FULL, m);
+        for (u32 base = 0; base < m_max; base += L * CH) {
+            double cv[CH];
+            u32 cb = 0;
+#pragma unroll
+            for (int c = 0; c < CH; ++c) {
+                cv[c] = f.canon(bx[c]);
+                const u32 i = base + L * c + gl;
+                const u32 gb = (__ballot_sync(FULL, !bdone && i > 0 && i < m && cv[c] == tv) >> gshift) & gbits;
+                if (gb && !cb) cb = base + L * c + __ffs(gb) - 1;
+            }
+            const u32 lim = cb ? cb : m;
+#pragma unroll
+            for (int c = 0; c < CH; ++c)
+                if (!bdone && base + L * c + gl < lim) h_insert(tab, mask, shift, hkey_canon(cv[c]));
+            if (cb && !bdone) {
+                cyc = cb;
+                baby_done = cb;
+            }
+            bdone = bdone || cb != 0 || base + L * CH >= m;
+            if (__all_sync(FULL, bdone)) break;
+#pragma unroll
+            for (int c = 0; c < CH; ++c) bx[c] = f.mul(bx[c], Bstep);
+        }
+        __syncwarp();
+
+        u64 best = ~0ull;
+        // a cycle: the j in [1, cyc) with G0 == t B^(cyc - j)
+        {
+            const int i = gfind_baby<L>(f, tbl, BL, 1, cyc, G0, cyc != 0, gl, gshift, gbits);
+            if (cyc && i > 0) best = cyc - (u32)i;
+        }
+        const u32 G = (active && !cyc && jc > 1) ? (jc - 1 + m - 1) / m : 0;   // g = 1..G covers j in [1, G*m]
+        u32 giant_done = G;
+        bool gdone = G == 0;
+        const u32 G_max = __reduce_max_sync(FULL, G);
+        for (u32 base = 0; base < G_max; base += L * CH) {
+            u32 hs[CH];
+            bool flag = false;
+#pragma unroll
+            for (int c = 0; c < CH; ++c) {
+                hs[c] = hkey_canon(f.canon(gx[c]));
+                const u32 slot = tab[hs[c] >> shift];
+                flag |= !gdone && ((((slot ^ hfp(hs[c])) & 0x7FFFu) == 0) | ((slot & 0x8000u) != 0));
+            }
+            if (__any_sync(FULL, flag)) {
+                u32 real = 0;
+#pragma unroll
+                for (int c = 0; c < CH; ++c)
+                    if (!gdone && base + L * c + gl + 1 <= G && h_contains(tab, mask, shift, hs[c])) real |= 1u << c;
+                u64 jb = ~0ull;
+#pragma unroll
+                for (int c = 0; c < CH; ++c) {
+                    u32 gb = (__ballot_sync(FULL, (real >> c) & 1u) >> gshift) & gbits;
+                    const double cvc = f.canon(gx[c]);
+                    while (__any_sync(FULL, gb != 0 && jb == ~0ull)) {
+                        const bool mine = gb != 0 && jb == ~0ull;
+                        const int src = mine ? __ffs(gb) - 1 : 0;
+                        const double v = __shfl_sync(FULL, cvc, gshift + (u32)src);
+                        const int i = gfind_baby<L>(f, tbl, BL, 0, m, v, mine, gl, gshift, gbits);
+                        if (mine) {
+                            gb &= gb - 1;
+                            if (i >= 0) jb = (u64)(base + L * c + (u32)src + 1) * m - (u64)i;
+                        }
+                    }
+                }
+                if (jb != ~0ull && !gdone) {
+                    best = jb;
+                    giant_done = min(G, base + L * CH);
+                    gdone = true;
+                }
+            }
+            gdone = gdone || base + L * CH >= G;
+            if (__all_sync(FULL, gdone)) break;
+#pragma unroll
+            for (int c = 0; c < CH; ++c) gx[c] = f.mul(gx[c], Gstep);
+        }
+        __syncwarp();
+        if (gl == 0 && active) {
+            if (best < e.jcount) emit_relation(e.p, e.n_first + best * e.L, 0, e.item, a.rel, a.rel_cap, ctr);
+            my_steps += (u64)baby_done + giant_done;
+        }
+    }
+    if (gl == 0 && my_steps) atomicAdd(&ctr->steps, (unsigned long long)my_steps);
 }
 
 // -------------------------------------------------------------- the order --
@@ -1843,7 +2045,8 @@ cudaError_t bsgs_reserve_smem(size_t smem) {
     std::lock_guard<std::mutex> g(lock);
     if (smem <= done[dev]) return cudaSuccess;
     for (auto kern : {k_bsgs<0, 0>, k_bsgs<1, 0>, k_bsgs<2, 0>, k_bsgs<4, 0>, k_bsgs<1, 1>, k_bsgs<2, 1>,
-                      k_bsgs<4, 1>, k_bsgs<1, 2>, k_bsgs<2, 2>, k_bsgs<4, 2>}) {
+                      k_bsgs<4, 1>, k_bsgs<1, 2>, k_bsgs<2, 2>, k_bsgs<4, 2>, k_bsgs_groups<8, 1>,
+                      k_bsgs_groups<8, 2>, k_bsgs_groups<16, 1>, k_bsgs_groups<16, 2>}) {
         err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (err != cudaSuccess) return err;
     }
@@ -1860,6 +2063,11 @@ cudaError_t launch_bsgs(const BsgsArgs& a, Counters* ctr, int grid, cudaStream_t
         return cudaGetLastError();
     };
     if (a.max_p >= kFp64Limit) return go(k_bsgs<0, 0>);
+    if (a.table_kind == 2 && (a.lanes == 8 || a.lanes == 16)) {
+        // groups of lanes per prime: FP64 arithmetic only (the caller checked p < 2^49)
+        if (a.lanes == 8) return a.chains == 1 ? go(k_bsgs_groups<8, 1>) : go(k_bsgs_groups<8, 2>);
+        return a.chains == 1 ? go(k_bsgs_groups<16, 1>) : go(k_bsgs_groups<16, 2>);
+    }
     if (a.table_kind == 2) {
         if (a.chains == 4) return go(k_bsgs<4, 2>);
         if (a.chains == 1) return go(k_bsgs<1, 2>);

@@ -100,6 +100,8 @@ struct BsgsArgs {
     u64 max_p;                 // largest p of the entries (>= 2^49: integer solve)
     u32 table_kind;            // FP64 solve: 0 = fingerprint words, 1 = 32-bit slots, 2 = 16-bit slots
     u32 load_shift;            // table kind 2: at most 2^-load_shift of a prime's slots are used
+    u32 lanes;                 // table kind 2: lanes per prime, 32 (a warp) or 16 / 8 (groups; every
+                               // entry must have p < 2^49, max_p > 0 and < 2^49 or the caller's guarantee)
 };
 constexpr u32 kDefaultLoadShift = 2;
 cudaError_t launch_bsgs(const BsgsArgs& a, Counters* ctr, int grid, cudaStream_t s);

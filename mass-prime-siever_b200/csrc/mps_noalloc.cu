@@ -208,7 +208,7 @@ int run_pass(unsigned char* base, u64 lo, u64 hi, const DevItem& d, u32 tbits, i
     Counters h;
     if (cudaMemcpyAsync(&h, ctr, sizeof(Counters), cudaMemcpyDeviceToHost, s) != cudaSuccess) return MPS_E_CUDA;
     if (cudaStreamSynchronize(s) != cudaSuccess) return MPS_E_CUDA;
-    if (h.status & kStatusOrderFailed) return MPS_E_CUDA;
+    if (h.status & (kStatusOrderFailed | kStatusBadLaunch)) return MPS_E_CUDA;
     if (h.status & (kStatusSurvivorOverflow | kStatusEntryOverflow | kStatusRelationOverflow)) {
         // denser than the scratch holds: split the range (no allocation)
         if (hi - lo < 64) return MPS_E_CAPACITY;

@@ -39,14 +39,14 @@ def test_cpu_chunking_keeps_every_thread_busy(monkeypatch):
 
 
 def test_tuning_summary():
-    reps = [dict(table_kind=2, load_shift=2, chains=2, warps=4, seg_words=2048, best_ns_per_prime=1.0,
+    reps = [dict(table_kind=2, load_shift=2, chains=2, warps=4, seg_words=2048, lanes=32, best_ns_per_prime=1.0,
                  default_ns_per_prime=1.5),
-            dict(table_kind=2, load_shift=2, chains=2, warps=4, seg_words=2048, best_ns_per_prime=2.0,
+            dict(table_kind=2, load_shift=2, chains=2, warps=4, seg_words=2048, lanes=32, best_ns_per_prime=2.0,
                  default_ns_per_prime=2.0),
-            dict(table_kind=0, load_shift=2, chains=4, warps=8, seg_words=4096, best_ns_per_prime=1.0,
+            dict(table_kind=0, load_shift=2, chains=4, warps=8, seg_words=4096, lanes=32, best_ns_per_prime=1.0,
                  default_ns_per_prime=1.2)]
     s = bench.tuning_summary(reps, 3.0)
-    assert s["classes"] == 3 and s["choices"] == {"kind2/load2^-2/ch2/w4/seg2048": 2, "kind0/ch4/w8/seg4096": 1}
+    assert s["classes"] == 3 and s["choices"] == {"kind2/load2^-2/lanes32/ch2/w4/seg2048": 2, "kind0/ch4/w8/seg4096": 1}
     assert s["bsgs_gain_vs_default"]["max"] == 1.5 and s["bsgs_gain_vs_default"]["min"] == 1.0
     assert bench.tuning_summary([], 0.0)["bsgs_gain_vs_default"] is None
 

@@ -127,7 +127,8 @@ def test_c1_prime_count(siever, golden):
     dict(chains=1), dict(chains=4), dict(table_bits=7, max_baby=256), dict(graphs_off=1),
     dict(table_kind=2), dict(table_kind=2, chains=1), dict(table_kind=2, chains=4), dict(table_kind=2, load_shift=3),
     dict(table_kind=2, load_shift=1, table_bits=7), dict(table_kind=2, bsgs_warps=8), dict(class_modulus=1),
-    dict(class_modulus=1, plain=1),
+    dict(class_modulus=1, plain=1), dict(table_kind=2, lanes=16), dict(table_kind=2, lanes=8, chains=1),
+    dict(table_kind=2, lanes=8, bsgs_warps=8), dict(table_kind=2, lanes=16, load_shift=3, plain=1),
 ])
 def test_tunings_give_identical_relations(mps_lib, oracle, tuning):
     specs = [(2, -25, 10**10, 10**10 + 4_000_000, 3_600_000, 5_000_000, 2, 1),
