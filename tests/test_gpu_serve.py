@@ -102,7 +102,9 @@ def test_admission_waits_for_a_reservation(mps_lib, golden):
 
 def test_item_larger_than_the_pool_fails(mps_lib, golden):
     case = next(c for c in golden["cases"] if c["name"] == "c2_low")
-    with mps_lib.Server(0, mem_budget_bytes=4096) as sv:
+    # a 16 KB pool: c2_low's reservation (~160 KB) never fits, an item with no
+    # in-class exponent (the 256-relation minimum, 8 KB) does
+    with mps_lib.Server(0, mem_budget_bytes=16384) as sv:
         t = sv.submit(mps_lib.make_item(*case["item"]))
         with pytest.raises(mps_lib.MpsError) as e:
             sv.wait(t)
