@@ -74,9 +74,10 @@ typedef struct mps_tuning {
     uint32_t graphs_off;        /* 1: launch waves directly instead of replaying CUDA graphs   */
     uint32_t table_kind;        /* BSGS table: 0 = four 16-bit fingerprints per 64-bit word,
                                    1 = one 32-bit key per slot, 2 = one 16-bit fingerprint
-                                   per slot, read with one 16-bit load per probe               */
-    uint32_t load_shift;        /* table kind 2: a prime's table is at least 2^load_shift times
-                                   its baby-step count (0: 2)                                  */
+                                   per slot, read with one 16-bit load per probe, 3 = the
+                                   words of 0 keyed from the FP64 pipe (no integer hash)       */
+    uint32_t load_shift;        /* table kinds 2 and 3: a prime's table has at least
+                                   2^load_shift slots per baby step (0: 2)                      */
     uint32_t lanes;             /* table kind 2: lanes per prime, 32, 16 or 8 (0: 32); groups of
                                    16 or 8 solve 2 or 4 primes per warp, for p < 2^49          */
     uint32_t reserved[2];

@@ -243,13 +243,14 @@ u32 groups_log(const LaunchCfg& g) { return g.kind == 2 ? (g.lanes == 8 ? 2 : g.
 u32 table_holds(const LaunchCfg& g, u32 tb) {
     if (g.kind == 0) return 1u << (tb - 1);
     if (g.kind == 2) return std::max<u32>(1u << (tb + 1 - g.load_shift) >> groups_log(g), 1);
+    if (g.kind == 3) return 1u << (tb + 1 - std::max<u32>(g.load_shift, 2));   // four slots a word
     return std::max<u32>((1u << tb) / 5, 1);
 }
 
 // Room for a prime's keys (load at most 1/2 in 16-bit slots): fingerprint
 // words hold four keys each, 32-bit slots one.
 u32 table_room(const LaunchCfg& g, u32 tb) {
-    if (g.kind == 0) return 1u << tb;
+    if (g.kind == 0 || g.kind == 3) return 1u << tb;
     if (g.kind == 2) return (1u << tb) >> groups_log(g);
     return (1u << tb) - 1;
 }
@@ -265,7 +266,7 @@ u32 table_room(const LaunchCfg& g, u32 tb) {
 // 2^-load_shift of them (up to 12 bits, 16 KB per warp, when load_shift > 2).
 void table_for(const mps_ctx* c, const LaunchCfg& g, u64 K, u32* tbits, u32* max_baby) {
     const u64 m_opt = (u64)std::ceil(std::sqrt((double)std::max<u64>(K, 1)));
-    const u32 top = g.kind == 2 && g.load_shift > 2 ? 12 : 11;
+    const u32 top = (g.kind == 2 || g.kind == 3) && g.load_shift > 2 ? 12 : 11;
     u32 tb = c->tun.table_bits;
     if (tb == 0) {
         tb = 6;
@@ -1651,14 +1652,14 @@ int mps_autotune(mps_ctx* c, const mps_item* items, size_t n_items, mps_tune_rep
     constexpr u64 kCalibSpan = 1ull << 25;
     const LaunchCfg base = default_cfg(c);
     std::vector<LaunchCfg> cands{base};
-    for (u32 kind : {0u, 2u})
+    for (u32 kind : {0u, 3u})
         for (u32 ls : {2u, 3u}) {
-            if (kind != 2 && ls != 2) continue;
+            if (kind == 0 && ls != 2) continue;
             for (u32 ch : {1u, 2u, 4u})
                 for (u32 w : {4u, 8u}) {
                     LaunchCfg g;
                     g.kind = kind;
-                    g.load_shift = kind == 2 ? ls : base.load_shift;
+                    g.load_shift = kind == 3 ? ls : base.load_shift;
                     g.chains = ch;
                     g.warps = w;
                     if (g != base) cands.push_back(g);
@@ -1801,7 +1802,7 @@ int mps_tune_load(mps_ctx* c, const char* path) {
     double ns;
     while (std::fscanf(f, "%llu %u %u %u %u %u %u %lf", &key, &kind, &ls, &ch, &w, &sw, &lanes, &ns) == 8) {
         // only configurations the kernels are built for
-        if (kind > 2 || ls < 1 || ls > 4 || (ch != 1 && ch != 2 && ch != 4) || w < 1 || w > 8 ||
+        if (kind > 3 || ls < 1 || ls > 4 || (ch != 1 && ch != 2 && ch != 4) || w < 1 || w > 8 ||
             (sw != 1024 && sw != 2048 && sw != 4096) || (lanes != 32 && lanes != 16 && lanes != 8) ||
             (lanes != 32 && (kind != 2 || ch == 4)))
             continue;

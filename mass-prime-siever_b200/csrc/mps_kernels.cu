@@ -1384,11 +1384,167 @@ __device__ u64 solve_fp64h(const Entry& e, unsigned short* tab, u32 tbits, u32 l
     return best < e.jcount ? best : ~0ull;
 }
 
+// ---- the FP64 solve with fingerprint words keyed from the FP64 pipe ----
+//
+// The table of solve_fp64q (four 16-bit fingerprints per 64-bit word, bit 15
+// of a half marks it used, bit 14 of half 0 is the word's overflow bit), with
+// the key taken from the canonical residue itself: x + 2^52 (one FP64 add)
+// holds x in its low mantissa bits, so the low 32 bits of x come out of the
+// register for free.  The home word is the low tw bits of x (a residue spread
+// over [0, p)), the fingerprint 14 high bits of a multiplicative hash.  The
+// next giant value is multiplied before the probe of the current one, so the
+// multiply's latency overlaps the shared-memory load and the vote.  A word
+// holds at most 2^-word_shift keys on average (word_shift 0: one key per word).
+
+__device__ __forceinline__ u32 xlow(const Fp64& f, double v, double two52) {   // low 32 bits of canon(v)
+    double u = __dadd_rn(v, two52);
+    if (v < 0.0) u = __dadd_rn(u, f.p);
+    return (u32)__double2loint(u);
+}
+
+// The fingerprint: bits 18..31 of lo * an odd constant (an integer multiply-add,
+// which runs on the FMA pipe), so that residues below 2^32 still spread.
+__device__ __forceinline__ u32 xpattern(u32 lo) { return (((lo * kHashMul) >> 18) & 0x3FFFu) | 0x8000u; }
+
+template <int CH>
+__device__ u64 solve_fp64x(const Entry& e, unsigned long long* tab, u32 tbits, u32 load_shift, u64* steps_out) {
+    const u32 lane = threadIdx.x & 31;
+    const u32 word_shift = load_shift > 2 ? load_shift - 2 : 0;   // slot load 2^-load_shift, four slots a word
+    const double two52 = 4503599627370496.0;
+    Fp64 f;
+    f.init(e.p);
+    const u32 m = e.m;
+    const u32 jc = (u32)e.jcount;                      // jcount <= 10^7
+    // 2^tw words for m keys, within the launch's 2^(tbits-1) words (tw <= 16 keeps home and fingerprint apart)
+    const u32 tw = min(tbits - 1, max(5u, 32u - __clz(max(m, 2u) - 1) + word_shift));
+    const u32 mask = (1u << tw) - 1;
+    const double B = (double)e.B, Bm = (double)e.Bm, tv = (double)e.t, G0 = (double)e.G0;
+
+    double xb = B, xg = Bm;                            // B^(l+1), Bm^(l+1)
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const double yb = __shfl_up_sync(FULL, xb, off), yg = __shfl_up_sync(FULL, xg, off);
+        if (lane >= (u32)off) {
+            xb = f.mul(xb, yb);
+            xg = f.mul(xg, yg);
+        }
+    }
+    const double B32 = __shfl_sync(FULL, xb, 31), Bm32 = __shfl_sync(FULL, xg, 31);
+    double bl = __shfl_up_sync(FULL, xb, 1);
+    if (lane == 0) bl = 1.0;
+    double Bstep = B32, Gstep = Bm32;                  // B^(32 CH), Bm^(32 CH)
+#pragma unroll
+    for (int c = 1; c < CH; c <<= 1) {
+        Bstep = f.mul(Bstep, Bstep);
+        Gstep = f.mul(Gstep, Gstep);
+    }
+    const double tbl = f.mul(tv, bl);
+    double bx[CH], gx[CH];
+    bx[0] = tbl;
+    gx[0] = f.mul(G0, xg);
+#pragma unroll
+    for (int c = 1; c < CH; ++c) {
+        bx[c] = f.mul(bx[c - 1], B32);
+        gx[c] = f.mul(gx[c - 1], Bm32);
+    }
+
+    uint4* t4 = reinterpret_cast<uint4*>(tab);
+    for (u32 k = lane; k <= mask / 2; k += 32) t4[k] = make_uint4(0, 0, 0, 0);
+    __syncwarp();
+
+    // baby steps, stopping at a cycle B^d == 1 (d < m)
+    u32 cyc = 0, baby_done = m;
+    for (u32 base = 0; base < m; base += 32 * CH) {
+        double cv[CH], nb[CH];
+        u32 cb = 0;
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            cv[c] = f.canon(bx[c]);
+            nb[c] = f.mul(bx[c], Bstep);
+            const u32 i = base + 32 * c + lane;
+            const u32 bc = __ballot_sync(FULL, i > 0 && i < m && cv[c] == tv);
+            if (bc && !cb) cb = base + 32 * c + __ffs(bc) - 1;
+        }
+        const u32 lim = cb ? cb : m;
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            const u32 i = base + 32 * c + lane;
+            if (i < lim) {
+                const u32 lo = (u32)__double2loint(__dadd_rn(cv[c], two52));
+                fq_insert(tab, mask, lo & mask, xpattern(lo));
+            }
+        }
+        if (cb) {
+            cyc = cb;
+            baby_done = cb;
+            break;
+        }
+#pragma unroll
+        for (int c = 0; c < CH; ++c) bx[c] = nb[c];
+    }
+    __syncwarp();
+
+    u64 best = ~0ull;
+    u32 giant_done = 0;
+    if (cyc) {
+        const int i = ffind_baby(f, tbl, B32, 1, cyc, G0);
+        if (i > 0) best = cyc - (u32)i;
+    } else {
+        const u32 G = (jc - 1 + m - 1) / m;            // g = 1..G covers j in [1, G*m]
+        giant_done = G;
+        const uint2* t2 = reinterpret_cast<const uint2*>(tab);
+        for (u32 base = 0; base < G; base += 32 * CH) {
+            u32 los[CH];
+            double nx[CH];
+            u32 cand = 0;
+#pragma unroll
+            for (int c = 0; c < CH; ++c) {
+                los[c] = xlow(f, gx[c], two52);
+                nx[c] = f.mul(gx[c], Gstep);              // the next value, independent of the probe
+                const uint2 w = t2[los[c] & mask];
+                cand |= fq_candidate(w.x, w.y, xpattern(los[c])) ? (1u << c) : 0u;
+            }
+            if (__any_sync(FULL, cand)) {
+                u32 real = 0;
+#pragma unroll
+                for (int c = 0; c < CH; ++c)
+                    if (((cand >> c) & 1u) && base + 32 * c + lane + 1 <= G &&
+                        fq_contains(tab, mask, los[c] & mask, xpattern(los[c])))
+                        real |= 1u << c;
+                u64 jb = ~0ull;
+#pragma unroll
+                for (int c = 0; c < CH; ++c) {
+                    u32 bb = __ballot_sync(FULL, (real >> c) & 1u);
+                    while (bb && jb == ~0ull) {
+                        const int src = __ffs(bb) - 1;
+                        bb &= bb - 1;
+                        const double v = __shfl_sync(FULL, f.canon(gx[c]), src);
+                        const u64 g = base + 32 * c + (u32)src + 1;
+                        const int i = ffind_baby(f, tbl, B32, 0, m, v);
+                        if (i >= 0) jb = g * m - (u64)i;
+                    }
+                }
+                if (jb != ~0ull) {
+                    best = jb;
+                    giant_done = min(G, base + 32 * CH);
+                    break;
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < CH; ++c) gx[c] = nx[c];
+        }
+    }
+    __syncwarp();
+    if (steps_out) *steps_out = (u64)baby_done + giant_done;
+    return best < e.jcount ? best : ~0ull;
+}
+
 template <int CH, int QT>
 __device__ __forceinline__ u64 solve_any(const Entry& e, void* tab, u32 tbits, u32 load_shift, u64* steps) {
     if (CH == 0 || e.p >= kFp64Limit) return solve_entry<FieldM>(e, (unsigned short*)tab, tbits + 1, steps);
     if (QT == 0) return solve_fp64q<CH ? CH : 1>(e, (unsigned long long*)tab, tbits, steps);
     if (QT == 2) return solve_fp64h<CH ? CH : 1>(e, (unsigned short*)tab, tbits, load_shift, steps);
+    if (QT == 3) return solve_fp64x<CH ? CH : 1>(e, (unsigned long long*)tab, tbits, load_shift, steps);
     return solve_fp64<CH ? CH : 1>(e, (u32*)tab, tbits, steps);
 }
 
@@ -1397,7 +1553,7 @@ __device__ __forceinline__ u64 solve_any(const Entry& e, void* tab, u32 tbits, u
 template <int CH, int QT>
 __device__ __forceinline__ bool fits_table(const Entry& e, u32 tbits) {
     if (CH == 0 || e.p >= kFp64Limit) return e.m <= (1u << tbits);          // 2^(tbits+1) 16-bit slots
-    if (QT == 0) return e.m <= (1u << tbits);                               // 2^(tbits-1) words of four
+    if (QT == 0 || QT == 3) return e.m <= (1u << tbits);                    // 2^(tbits-1) words of four
     if (QT == 2) return e.m <= (1u << tbits);                               // 2^(tbits+1) 16-bit slots
     return e.m < (1u << tbits);                                            // 2^tbits 32-bit slots
 }
@@ -1971,9 +2127,9 @@ __global__ void k_bsgs_direct(const u64* cases, u64* j_out, u64 count, u32 tbits
     } else {
         u32 m = (u32)isqrt_ceil_dev(e.jcount);
         // the table loads of the sieving path
-        const u32 cap = min(kMaxBaby, table_kind == 0   ? 1u << (tbits - 1)
-                                      : table_kind == 2 ? 1u << (tbits + 1 - kDefaultLoadShift)
-                                                        : max(1u, (1u << tbits) / 5));
+        const u32 cap = min(kMaxBaby, table_kind == 0 || table_kind == 3 ? 1u << (tbits - 1)
+                                      : table_kind == 2                    ? 1u << (tbits + 1 - kDefaultLoadShift)
+                                                                           : max(1u, (1u << tbits) / 5));
         if (m > cap) m = cap;
         e.m = m;
         Mont M;
@@ -1983,6 +2139,7 @@ __global__ void k_bsgs_direct(const u64* cases, u64* j_out, u64 count, u32 tbits
         if (e.p >= kFp64Limit) result = solve_any<0, 0>(e, smem32, tbits, kDefaultLoadShift, nullptr);
         else if (table_kind == 0) result = solve_any<2, 0>(e, smem32, tbits, kDefaultLoadShift, nullptr);
         else if (table_kind == 2) result = solve_any<2, 2>(e, smem32, tbits, kDefaultLoadShift, nullptr);
+        else if (table_kind == 3) result = solve_any<2, 3>(e, smem32, tbits, 0, nullptr);
         else result = solve_any<2, 1>(e, smem32, tbits, kDefaultLoadShift, nullptr);
     }
     if (threadIdx.x == 0) j_out[idx] = result;
@@ -2045,7 +2202,8 @@ cudaError_t bsgs_reserve_smem(size_t smem) {
     std::lock_guard<std::mutex> g(lock);
     if (smem <= done[dev]) return cudaSuccess;
     for (auto kern : {k_bsgs<0, 0>, k_bsgs<1, 0>, k_bsgs<2, 0>, k_bsgs<4, 0>, k_bsgs<1, 1>, k_bsgs<2, 1>,
-                      k_bsgs<4, 1>, k_bsgs<1, 2>, k_bsgs<2, 2>, k_bsgs<4, 2>, k_bsgs_groups<8, 1>,
+                      k_bsgs<4, 1>, k_bsgs<1, 2>, k_bsgs<2, 2>, k_bsgs<4, 2>, k_bsgs<1, 3>, k_bsgs<2, 3>,
+                      k_bsgs<4, 3>, k_bsgs_groups<8, 1>,
                       k_bsgs_groups<8, 2>, k_bsgs_groups<16, 1>, k_bsgs_groups<16, 2>}) {
         err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (err != cudaSuccess) return err;
@@ -2067,6 +2225,11 @@ cudaError_t launch_bsgs(const BsgsArgs& a, Counters* ctr, int grid, cudaStream_t
         // groups of lanes per prime: FP64 arithmetic only (the caller checked p < 2^49)
         if (a.lanes == 8) return a.chains == 1 ? go(k_bsgs_groups<8, 1>) : go(k_bsgs_groups<8, 2>);
         return a.chains == 1 ? go(k_bsgs_groups<16, 1>) : go(k_bsgs_groups<16, 2>);
+    }
+    if (a.table_kind == 3) {
+        if (a.chains == 4) return go(k_bsgs<4, 3>);
+        if (a.chains == 1) return go(k_bsgs<1, 3>);
+        return go(k_bsgs<2, 3>);
     }
     if (a.table_kind == 2) {
         if (a.chains == 4) return go(k_bsgs<4, 2>);

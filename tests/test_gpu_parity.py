@@ -69,7 +69,7 @@ def _bsgs_cases(seed, count):
 
 
 @pytest.mark.parametrize("table_bits", [5, 6, 9, 12, 13])
-@pytest.mark.parametrize("table_kind", [0, 1, 2])
+@pytest.mark.parametrize("table_kind", [0, 1, 2, 3])
 def test_bsgs_smallest_j(mps_lib, oracle, table_bits, table_kind):
     cases = _bsgs_cases(100 + table_bits, 400)
     with mps_lib.Siever(0, table_kind=table_kind) as s:
@@ -129,6 +129,8 @@ def test_c1_prime_count(siever, golden):
     dict(table_kind=2, load_shift=1, table_bits=7), dict(table_kind=2, bsgs_warps=8), dict(class_modulus=1),
     dict(class_modulus=1, plain=1), dict(table_kind=2, lanes=16), dict(table_kind=2, lanes=8, chains=1),
     dict(table_kind=2, lanes=8, bsgs_warps=8), dict(table_kind=2, lanes=16, load_shift=3, plain=1),
+    dict(table_kind=3), dict(table_kind=3, chains=4), dict(table_kind=3, load_shift=3, chains=1),
+    dict(table_kind=3, load_shift=3, bsgs_warps=8, plain=1),
 ])
 def test_tunings_give_identical_relations(mps_lib, oracle, tuning):
     specs = [(2, -25, 10**10, 10**10 + 4_000_000, 3_600_000, 5_000_000, 2, 1),
