@@ -85,6 +85,7 @@ struct Counters {
     unsigned long long status;     u64 pad4[7];   // nonzero: an error bit set by a kernel
     unsigned long long primes;     u64 pad5[7];   // prime count (counting kernel only)
     unsigned long long steps;      u64 pad6[7];   // baby + giant steps executed by the BSGS
+    unsigned long long prep_next;  u64 pad7[7];   // next survivor the prep's warps claim
 };
 
 // Status bits a kernel may set (host turns them into error codes).

@@ -536,7 +536,6 @@ __device__ __forceinline__ bool stage1(u64 p, const PrepArgs& a) {
 }
 
 constexpr u32 kPrepThreads = 256;
-constexpr u32 kPrepBatch = 1024;
 constexpr u32 kWalk = 48;                              // stage-2 walk before deferring
 
 // Warp-aggregated push onto a shared-memory queue.
@@ -551,133 +550,167 @@ __device__ __forceinline__ u32 queue_slot(u32* count, bool want) {
     return base + __popc(bal & ((1u << lane) - 1));
 }
 
-// The prep: one persistent kernel; each block takes batches of kPrepBatch
-// survivors through four stages separated by shared-memory queues, so that
-// every stage runs with full warps.
+// The prep: one persistent kernel without block barriers.  Every warp claims
+// 32 survivors at a time and carries them through the stages on its own,
+// with three warp-private queues in shared memory between the stages
+// (survivors that passed stage 1; primes with their (d, r) for stage 3;
+// primes deferred to stage 2b).  A queue is drained whenever it holds 32
+// entries, so every stage runs with full warps, and a warp never waits for
+// another; the partial queues are drained at the end.  A queue never holds
+// more than 63 entries: a stage pushes at most 32 into a queue that held
+// fewer than 32.
+constexpr u32 kPrepWarps = kPrepThreads / 32;
+
+struct PrepQueues {
+    u64 p1[64];
+    u32 i1[64];
+    u64 p2[64];
+    u32 i2[64], d2[64], r2[64];
+    u64 pd[64];
+    u32 id[64];
+};
+
+// Appends the lanes with want to a warp queue of n entries (n warp-uniform).
+__device__ __forceinline__ void qpush(bool want, u32& n, u32* slot_out) {
+    const u32 lane = threadIdx.x & 31;
+    const u32 bal = __ballot_sync(FULL, want);
+    *slot_out = n + __popc(bal & ((1u << lane) - 1));
+    n += __popc(bal);
+}
+
+template <class F>
+__device__ __forceinline__ int split_in(const DevItem& it, u64 p, u32& d, u32& r) {
+    F f;
+    f.init(p);
+    const u64 bm = residue128(it.babs_hi, it.babs_lo, it.b_neg, p);
+    const u64 t = p - residue128(it.cabs_hi, it.cabs_lo, it.c_neg, p);
+    return power_split(f, p, bm, t, it, kWalk, d, r);
+}
+
+template <class F>
+__device__ __forceinline__ bool split_pp_in(const DevItem& it, u64 p, u32& d, u32& r) {
+    F f;
+    f.init(p);
+    const u64 bm = residue128(it.babs_hi, it.babs_lo, it.b_neg, p);
+    const u64 t = p - residue128(it.cabs_hi, it.cabs_lo, it.c_neg, p);
+    return power_split_pp(f, p, bm, t, it, d, r);
+}
+
+template <class F>
+__device__ __forceinline__ void setup_in(const DevItem& it, u64 p, u32 d, u32 r, const PrepArgs& a, Counters* ctr) {
+    F f;
+    f.init(p);
+    const u64 bm = residue128(it.babs_hi, it.babs_lo, it.b_neg, p);
+    const u64 t = p - residue128(it.cabs_hi, it.cabs_lo, it.c_neg, p);
+    bsgs_setup(f, p, bm, t, it, d, r, a, ctr);
+}
+
 __global__ void __launch_bounds__(kPrepThreads) k_prep(PrepArgs a, Counters* ctr) {
-    __shared__ u64 q_p[kPrepBatch];
-    __shared__ u32 q_item[kPrepBatch];
-    __shared__ u32 q_d[kPrepBatch];                    // d, r after stage 2
-    __shared__ u32 q_r[kPrepBatch];
-    __shared__ u64 d_p[kPrepBatch];                    // deferred to stage 2b
-    __shared__ u32 d_item[kPrepBatch];
-    __shared__ u32 n_q, n_q2, n_d;
-    __shared__ u64 q2_p[kPrepBatch];
-    __shared__ u32 q2_item[kPrepBatch];
-    const u64 n = min((u64)*(volatile unsigned long long*)&ctr->survivors, a.surv_cap);
-    const u32 tid = threadIdx.x;
-    for (u64 b0 = (u64)blockIdx.x * kPrepBatch; b0 < n; b0 += (u64)gridDim.x * kPrepBatch) {
-        const u32 nb = (u32)min((u64)kPrepBatch, n - b0);
-        if (tid == 0) n_q = n_q2 = n_d = 0;
-        __syncthreads();
-        // stage 1: special cases, then the base-2 strong test
-        for (u32 k = tid; k < kPrepBatch; k += kPrepThreads) {
-            bool keep = false;
-            u64 p = 0;
-            u32 item = a.item0;
-            if (k < nb) {
-                p = a.surv[b0 + k];
-                if (a.surv_item) item = a.surv_item[b0 + k];
-                u64 bm, t;
-                if (prep_special(p, a.items[item], a, ctr, bm, t) && !qr_reject(p, a.items[item]))
-                    keep = p < kFp64Limit ? stage1<FieldF>(p, a) : stage1<FieldM>(p, a);
+    __shared__ PrepQueues qs[kPrepWarps];
+    PrepQueues& Q = qs[threadIdx.x >> 5];
+    const u32 lane = threadIdx.x & 31;
+    const u64 n_surv = min((u64)*(volatile unsigned long long*)&ctr->survivors, a.surv_cap);
+    u32 n1 = 0, n2 = 0, nd = 0;                          // queue lengths (warp-uniform)
+    bool inputs = true;
+    for (;;) {
+        if (n2 >= 32 || (!inputs && n1 == 0 && nd == 0 && n2 > 0)) {
+            // stage 3: class combination and the BSGS set-up
+            const u32 cnt = min(n2, 32u);
+            if (lane < cnt) {
+                const u32 k = n2 - cnt + lane;
+                const u64 p = Q.p2[k];
+                const DevItem& it = a.items[Q.i2[k]];
+                if (p < kFp64Limit) setup_in<FieldF>(it, p, Q.d2[k], Q.r2[k], a, ctr);
+                else setup_in<FieldM>(it, p, Q.d2[k], Q.r2[k], a, ctr);
             }
-            const u32 s = queue_slot(&n_q, keep);
-            if (keep) {
-                q_p[s] = p;
-                q_item[s] = item;
-            }
+            n2 -= cnt;
+            __syncwarp();
+            continue;
         }
-        __syncthreads();
-        // stage 2: power-residue split with a short walk
-        const u32 nq = n_q;
-        for (u32 k = tid; k < ((nq + 31) & ~31u); k += kPrepThreads) {
-            int res = 0;
-            u32 d = 1, r = 0;
-            u64 p = 0;
-            u32 item = 0;
-            if (k < nq) {
-                p = q_p[k];
-                item = q_item[k];
-                const DevItem& it = a.items[item];
-                const u64 bm = residue128(it.babs_hi, it.babs_lo, it.b_neg, p);
-                const u64 cm_ = residue128(it.cabs_hi, it.cabs_lo, it.c_neg, p);
-                const u64 t = p - cm_;
-                if (p < kFp64Limit) {
-                    FieldF f;
-                    f.init(p);
-                    res = power_split(f, p, bm, t, it, kWalk, d, r);
-                } else {
-                    FieldM f;
-                    f.init(p);
-                    res = power_split(f, p, bm, t, it, kWalk, d, r);
-                }
-            }
-            const u32 s2 = queue_slot(&n_q2, res == 1);
-            if (res == 1) {
-                q2_p[s2] = p;
-                q2_item[s2] = item;
-                q_d[s2] = d;
-                q_r[s2] = r;
-            }
-            const u32 sd = queue_slot(&n_d, res == 2);
-            if (res == 2) {
-                d_p[sd] = p;
-                d_item[sd] = item;
-            }
-        }
-        __syncthreads();
-        // stage 2b: long orders, one prime power at a time
-        const u32 nd = n_d;
-        for (u32 k = tid; k < ((nd + 31) & ~31u); k += kPrepThreads) {
+        if (nd >= 32 || (!inputs && n1 == 0 && nd > 0)) {
+            // stage 2b: long orders, one prime power at a time
+            const u32 cnt = min(nd, 32u);
             bool ok = false;
-            u32 d = 1, r = 0;
+            u32 d = 1, r = 0, item = 0;
             u64 p = 0;
-            u32 item = 0;
-            if (k < nd) {
-                p = d_p[k];
-                item = d_item[k];
+            if (lane < cnt) {
+                const u32 k = nd - cnt + lane;
+                p = Q.pd[k];
+                item = Q.id[k];
                 const DevItem& it = a.items[item];
-                const u64 bm = residue128(it.babs_hi, it.babs_lo, it.b_neg, p);
-                const u64 t = p - residue128(it.cabs_hi, it.cabs_lo, it.c_neg, p);
-                if (p < kFp64Limit) {
-                    FieldF f;
-                    f.init(p);
-                    ok = power_split_pp(f, p, bm, t, it, d, r);
-                } else {
-                    FieldM f;
-                    f.init(p);
-                    ok = power_split_pp(f, p, bm, t, it, d, r);
-                }
+                ok = p < kFp64Limit ? split_pp_in<FieldF>(it, p, d, r) : split_pp_in<FieldM>(it, p, d, r);
             }
-            const u32 s2 = queue_slot(&n_q2, ok);
+            nd -= cnt;
+            __syncwarp();
+            u32 s2;
+            qpush(ok, n2, &s2);
             if (ok) {
-                q2_p[s2] = p;
-                q2_item[s2] = item;
-                q_d[s2] = d;
-                q_r[s2] = r;
+                Q.p2[s2] = p;
+                Q.i2[s2] = item;
+                Q.d2[s2] = d;
+                Q.r2[s2] = r;
             }
+            __syncwarp();
+            continue;
         }
-        __syncthreads();
-        // stage 3: class combination and the BSGS set-up
-        const u32 nq2 = n_q2;
-        for (u32 k = tid; k < nq2; k += kPrepThreads) {
-            const u64 p = q2_p[k];
-            const DevItem& it = a.items[q2_item[k]];
-            const u64 bm = residue128(it.babs_hi, it.babs_lo, it.b_neg, p);
-            const u64 t = p - residue128(it.cabs_hi, it.cabs_lo, it.c_neg, p);
-            const u32 d = q_d[k], r = q_r[k];
-            if (p < kFp64Limit) {
-                FieldF f;
-                f.init(p);
-                bsgs_setup(f, p, bm, t, it, d, r, a, ctr);
-            } else {
-                FieldM f;
-                f.init(p);
-                bsgs_setup(f, p, bm, t, it, d, r, a, ctr);
+        if (n1 >= 32 || (!inputs && n1 > 0)) {
+            // stage 2: power-residue split with a short walk
+            const u32 cnt = min(n1, 32u);
+            int res = 0;
+            u32 d = 1, r = 0, item = 0;
+            u64 p = 0;
+            if (lane < cnt) {
+                const u32 k = n1 - cnt + lane;
+                p = Q.p1[k];
+                item = Q.i1[k];
+                const DevItem& it = a.items[item];
+                res = p < kFp64Limit ? split_in<FieldF>(it, p, d, r) : split_in<FieldM>(it, p, d, r);
             }
+            n1 -= cnt;
+            __syncwarp();
+            u32 s2, sd;
+            qpush(res == 1, n2, &s2);
+            qpush(res == 2, nd, &sd);
+            if (res == 1) {
+                Q.p2[s2] = p;
+                Q.i2[s2] = item;
+                Q.d2[s2] = d;
+                Q.r2[s2] = r;
+            } else if (res == 2) {
+                Q.pd[sd] = p;
+                Q.id[sd] = item;
+            }
+            __syncwarp();
+            continue;
         }
-        __syncthreads();
+        if (!inputs) break;
+        // stage 1: claim 32 survivors; special cases, the quadratic-character
+        // prefilter, then the base-2 strong test
+        u64 first = 0;
+        if (lane == 0) first = atomicAdd(&ctr->prep_next, 32ull);
+        first = __shfl_sync(FULL, first, 0);
+        if (first >= n_surv) {
+            inputs = false;
+            continue;
+        }
+        const u64 k = first + lane;
+        bool keep = false;
+        u64 p = 0;
+        u32 item = a.item0;
+        if (k < n_surv) {
+            p = a.surv[k];
+            if (a.surv_item) item = a.surv_item[k];
+            u64 bm, t;
+            if (prep_special(p, a.items[item], a, ctr, bm, t) && !qr_reject(p, a.items[item]))
+                keep = p < kFp64Limit ? stage1<FieldF>(p, a) : stage1<FieldM>(p, a);
+        }
+        u32 s1;
+        qpush(keep, n1, &s1);
+        if (keep) {
+            Q.p1[s1] = p;
+            Q.i1[s1] = item;
+        }
+        __syncwarp();
     }
 }
 
