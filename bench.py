@@ -335,7 +335,8 @@ def tuning_summary(reports: list[dict], seconds: float) -> dict:
     counts: dict[str, int] = {}
     for r in reports:
         key = (f"kind{r['table_kind']}" + (f"/load2^-{r['load_shift']}/lanes{r['lanes']}" if r["table_kind"] == 2
-                                           else "") + f"/ch{r['chains']}/w{r['warps']}/seg{r['seg_words']}")
+                                           else f"/fill{r.get('table_fill', 256)}/scale{r.get('baby_scale', 256)}")
+               + f"/ch{r['chains']}/w{r['warps']}/seg{r['seg_words']}")
         counts[key] = counts.get(key, 0) + 1
     gain = [r["default_ns_per_prime"] / r["best_ns_per_prime"] for r in reports if r["best_ns_per_prime"] > 0]
     return {"classes": len(reports), "seconds": seconds, "choices": counts,

@@ -80,7 +80,10 @@ typedef struct mps_tuning {
                                    2^load_shift slots per baby step (0: 2)                      */
     uint32_t lanes;             /* table kind 2: lanes per prime, 32, 16 or 8 (0: 32); groups of
                                    16 or 8 solve 2 or 4 primes per warp, for p < 2^49          */
-    uint32_t reserved[2];
+    uint32_t table_fill;        /* table kinds 0 and 3: at most table_fill/256 keys per 64-bit
+                                   word on average, 1..256 (0: 192)                            */
+    uint32_t baby_scale;        /* baby steps m = ceil(sqrt(j range) * baby_scale / 256) before
+                                   the table's cap, 1..1024 (0: 256, the square root)          */
 } mps_tuning;
 
 /* Counters of the last call (all chunks of it). */
@@ -200,8 +203,9 @@ int mps_serve_close(mps_server* sv);
  * in-class exponents), the class modulus, the decimal digits of P0 -- times
  * each candidate BSGS configuration (table kind, table load, lanes per prime,
  * chains per lane, warps per block) by the BSGS kernel's CUDA events on a calibration slice of
- * the item (its first 2^25 integers), then with the fastest the sieve's
- * segment size (1024, 2048 or 4096 words) by the sieve kernel's events;
+ * the item (its first 2^25 integers); with the fastest, the table fill and the
+ * baby/giant balance (baby_scale) the same way; then the sieve's segment size
+ * (1024, 2048 or 4096 words) by the sieve kernel's events;
  * checks that every candidate gives the same relations, and keeps the
  * fastest configuration for the class.  Later calls on items of a tuned class
  * use it (per item; a batched wave uses the configuration of its item with
@@ -216,6 +220,8 @@ typedef struct mps_tune_report {
     uint32_t table_kind, load_shift, chains, warps;   /* the BSGS configuration chosen   */
     uint32_t seg_words;           /* the sieve segment chosen (words of 32 odd numbers)  */
     uint32_t lanes;               /* lanes per prime chosen (32, or groups of 16 or 8)   */
+    uint32_t table_fill;          /* table load chosen (keys per word x 256)             */
+    uint32_t baby_scale;          /* baby-step scale chosen (x 256 of the square root)   */
     double   best_ns_per_prime;   /* BSGS time per prime reaching the BSGS, chosen       */
     double   default_ns_per_prime;/* the same under the context's tuning fields          */
     double   sieve_best_ms;       /* sieve time of the calibration slice, chosen segment */
@@ -224,7 +230,7 @@ typedef struct mps_tune_report {
 } mps_tune_report;
 int mps_autotune(mps_ctx* ctx, const mps_item* items, size_t n_items, mps_tune_report* out, size_t cap,
                  size_t* n_out);
-/* The tuned classes as text ("mps-tune 3" then one line per class); mps_open
+/* The tuned classes as text ("mps-tune 4" then one line per class); mps_open
  * loads the file named by the environment variable MPS_TUNE_CACHE, if set. */
 int mps_tune_save(const mps_ctx* ctx, const char* path);
 int mps_tune_load(mps_ctx* ctx, const char* path);

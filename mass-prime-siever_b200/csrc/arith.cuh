@@ -94,6 +94,18 @@ __device__ __forceinline__ u32 gcd32(u32 a, u32 b) {
     return a;
 }
 
+// a^-1 mod m for gcd(a, m) = 1, 0 <= a < m (extended Euclid; m == 1 gives 0).
+__device__ __forceinline__ u32 inv_mod32(u32 a, u32 m) {
+    u32 r0 = m, r1 = a;
+    long long s0 = 0, s1 = 1;                          // |s| <= m
+    while (r1) {
+        const u32 q = r0 / r1, r2 = r0 - q * r1;
+        const long long s2 = s0 - (long long)q * s1;
+        r0 = r1; r1 = r2; s0 = s1; s1 = s2;
+    }
+    return (u32)(s0 < 0 ? s0 + m : s0) % m;
+}
+
 // Jacobi symbol (a/n) for odd n < 2^32, a < n: the binary algorithm (strip
 // twos with (2/n) = -1 iff n == 3, 5 mod 8; swap with reciprocity, sign -1
 // iff both are 3 mod 4).  Returns 1, -1, or 0 when gcd(a, n) > 1.

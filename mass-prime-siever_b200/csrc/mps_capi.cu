@@ -63,9 +63,11 @@ const HostTables& host_tables() {
 struct LaunchCfg {
     u32 kind = 0, load_shift = kDefaultLoadShift, chains = 2, warps = 4, seg_words = kDefaultSegWords;
     u32 lanes = 32;     // lanes per prime (table kind 2: 32, or groups of 16 / 8 for p < 2^49)
+    u32 fill = kDefaultFill;           // table kinds 0 and 3: keys per word x 256, at most
+    u32 scale = kDefaultBabyScale;     // baby steps: ceil(sqrt(j range)) x scale / 256
     bool operator==(const LaunchCfg& o) const {
         return kind == o.kind && load_shift == o.load_shift && chains == o.chains && warps == o.warps &&
-               seg_words == o.seg_words && lanes == o.lanes;
+               seg_words == o.seg_words && lanes == o.lanes && fill == o.fill && scale == o.scale;
     }
     bool operator!=(const LaunchCfg& o) const { return !(*this == o); }
 };
@@ -215,6 +217,8 @@ LaunchCfg default_cfg(const mps_ctx* c) {
     const u32 lanes = c->tun.lanes;
     // groups of lanes exist for the 16-bit slot table with 1 or 2 chains
     g.lanes = g.kind == 2 && g.chains <= 2 && (lanes == 8 || lanes == 16) ? lanes : 32;
+    g.fill = c->tun.table_fill ? std::min<u32>(c->tun.table_fill, 256) : kDefaultFill;
+    g.scale = c->tun.baby_scale ? std::min<u32>(c->tun.baby_scale, 1024) : kDefaultBabyScale;
     return g;
 }
 
@@ -239,11 +243,13 @@ LaunchCfg cfg_for(const mps_ctx* c, u64 K, u64 cm, u64 P0) {
 // log2 of the primes a warp solves at once (lanes per prime 32, 16 or 8).
 u32 groups_log(const LaunchCfg& g) { return g.kind == 2 ? (g.lanes == 8 ? 2 : g.lanes == 16 ? 1 : 0) : 0; }
 
-// Keys a prime's table holds under configuration g with 4 << tb bytes per warp.
+// Keys a prime's table holds under configuration g with 4 << tb bytes per warp
+// (fingerprint words: at most fill/256 keys per word on average).
 u32 table_holds(const LaunchCfg& g, u32 tb) {
-    if (g.kind == 0) return 1u << (tb - 1);
+    const u32 fill = g.fill - 1 < 256 ? g.fill : 256;
+    if (g.kind == 0) return std::max<u32>(((1u << (tb - 1)) * fill) >> 8, 1);
     if (g.kind == 2) return std::max<u32>(1u << (tb + 1 - g.load_shift) >> groups_log(g), 1);
-    if (g.kind == 3) return 1u << (tb + 1 - std::max<u32>(g.load_shift, 2));   // four slots a word
+    if (g.kind == 3) return std::max<u32>(((1u << (tb + 1 - std::max<u32>(g.load_shift, 2))) * fill) >> 8, 1);
     return std::max<u32>((1u << tb) / 5, 1);
 }
 
@@ -303,6 +309,7 @@ int make_dev_item(mps_ctx* c, const mps_item* it, u32 index, DevItem* d, LaunchC
     u32 tb = 0, mb = 0;
     table_for(c, g, d->K, &tb, &mb);
     d->max_baby = mb;
+    d->baby_scale = g.scale;
     if (cfg) *cfg = g;
     return MPS_OK;
 }
@@ -396,6 +403,7 @@ int run_chunk(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, const LaunchCfg& g_it
     ba.warps_per_block = warps;
     ba.chains = g.chains;
     ba.table_kind = g.kind;
+    ba.fill = g.fill;
     ba.load_shift = g.load_shift;
     ba.lanes = g.lanes;
     ba.max_p = hi;
@@ -552,7 +560,7 @@ int slot_enqueue(mps_ctx* c, WaveSlot& w, u32 tbits, const LaunchCfg& g, bool ca
     BsgsArgs ba{};
     ba.ent = w.d_ent; ba.ent_cap = w.ent_cap; ba.rel = w.d_rel; ba.rel_cap = w.rel_cap; ba.tbits = tbits;
     ba.warps_per_block = warps; ba.persistent = 1; ba.chains = g.chains;
-    ba.table_kind = g.kind; ba.load_shift = g.load_shift; ba.lanes = g.lanes;
+    ba.table_kind = g.kind; ba.load_shift = g.load_shift; ba.lanes = g.lanes; ba.fill = g.fill;
     ba.max_p = 0;   // per-entry arithmetic
     OrderArgs oa{};
     oa.rel = w.d_rel; oa.rel_cap = w.rel_cap; oa.items = c->d_items; oa.tables = c->tables();
@@ -1327,6 +1335,7 @@ int mps_filter(mps_ctx* c, const uint64_t* primes, size_t n, const mps_item* ite
         ba.ent = c->d_ent; ba.ent_cap = c->ent_cap; ba.rel = c->d_rel; ba.rel_cap = c->rel_cap;
         ba.tbits = tbits; ba.warps_per_block = warps; ba.persistent = 1; ba.chains = g.chains; ba.table_kind = g.kind;
         ba.load_shift = g.load_shift;
+        ba.fill = g.fill;
         ba.lanes = for_range(g, *std::max_element(primes + off, primes + off + cnt) + 1).lanes;
         ba.max_p = *std::max_element(primes + off, primes + off + cnt);
         OrderArgs oa{};
@@ -1691,28 +1700,38 @@ int mps_autotune(mps_ctx* c, const mps_item* items, size_t n_items, mps_tune_rep
         LaunchCfg best = base;
         std::vector<RawRelation> first;
         // phase 1: the BSGS configuration by the BSGS kernel's time; phase 2: with
-        // it, the sieve's segment size by the sieve kernel's time
-        std::vector<LaunchCfg> segs;
-        for (u32 w : {1024u, 2048u, 4096u}) {
-            LaunchCfg g = base;
-            g.seg_words = w;
-            segs.push_back(g);
-        }
+        // it, the table fill and the baby-step scale (fingerprint words only);
+        // phase 3: the sieve's segment size by the sieve kernel's time
+        constexpr u32 kFills[] = {256u, 224u, 192u, 160u, 128u};
+        constexpr u32 kScales[] = {256u, 224u, 192u, 160u};
         const size_t n_bsgs = cands.size();
-        cands.insert(cands.end(), segs.begin(), segs.end());
-        for (size_t k = 0; k < cands.size(); ++k) {
-            LaunchCfg g = cands[k];
-            if (k >= n_bsgs) {                                  // phase 2 keeps the chosen BSGS settings
-                const u32 w = g.seg_words;
+        const size_t n_fill = n_bsgs + (sizeof(kFills) / sizeof(kFills[0])) * (sizeof(kScales) / sizeof(kScales[0]));
+        const size_t n_all = n_fill + 3;
+        size_t timed = 0;
+        for (size_t k = 0; k < n_all; ++k) {
+            LaunchCfg g;
+            if (k < n_bsgs) {
+                g = cands[k];
+            } else if (k < n_fill) {                            // phase 2 keeps the chosen BSGS settings
+                if (best.kind != 0 && best.kind != 3) continue;
+                const size_t f = (k - n_bsgs) / (sizeof(kScales) / sizeof(kScales[0]));
+                const size_t sc = (k - n_bsgs) % (sizeof(kScales) / sizeof(kScales[0]));
                 g = best;
-                g.seg_words = w;
+                g.fill = kFills[f];
+                g.scale = kScales[sc];
+                if (g == best) continue;
+            } else {                                            // phase 3 keeps the chosen BSGS settings
+                g = best;
+                g.seg_words = 1024u << (k - n_fill);
             }
             if (g.lanes != 32 && hi > kFp64Limit) continue;    // groups run the FP64 solve only
             u32 tb, mb;
             table_for(c, g, d.K, &tb, &mb);
             d.max_baby = mb;
+            d.baby_scale = g.scale;
             if (bsgs_smem_bytes(tb, g.warps) > c->smem_optin) continue;
             if (int r = upload_items(c, &d, 1)) return r;
+            ++timed;
             double ms = 0, sms = 0;
             for (int rep = 0; rep < 2; ++rep) {                 // the second run is timed
                 std::vector<RawRelation> rel;
@@ -1731,7 +1750,7 @@ int mps_autotune(mps_ctx* c, const mps_item* items, size_t n_items, mps_tune_rep
                     return fail(c, MPS_E_CUDA, "tuning candidates gave different relations");
                 }
             }
-            if (k < n_bsgs) {
+            if (k < n_fill) {
                 if (k == 0) base_ms = ms;
                 if (k == 0 || ms < best_ms) {
                     best_ms = ms;
@@ -1739,13 +1758,12 @@ int mps_autotune(mps_ctx* c, const mps_item* items, size_t n_items, mps_tune_rep
                 }
             } else {
                 if (g.seg_words == base.seg_words) sieve_base_ms = sms;
-                if (k == n_bsgs || sms < sieve_best_ms) {
+                if (k == n_fill || sms < sieve_best_ms) {
                     sieve_best_ms = sms;
                     best.seg_words = g.seg_words;
                 }
             }
         }
-        cands.resize(n_bsgs);
         const double per = entries ? 1e6 / (double)entries : 0.0;
         TuneEntry te;
         te.cfg = best;
@@ -1755,13 +1773,15 @@ int mps_autotune(mps_ctx* c, const mps_item* items, size_t n_items, mps_tune_rep
         rp.k_bits = (u32)(key >> 40);
         rp.mod = (u32)((key >> 8) & 4095);
         rp.p_digits = (u32)(key & 255);
-        rp.candidates = (u32)cands.size();
+        rp.candidates = (u32)timed;
         rp.table_kind = best.kind;
         rp.load_shift = best.load_shift;
         rp.chains = best.chains;
         rp.warps = best.warps;
         rp.seg_words = best.seg_words;
         rp.lanes = best.lanes;
+        rp.table_fill = best.fill;
+        rp.baby_scale = best.scale;
         rp.sieve_best_ms = sieve_best_ms;
         rp.sieve_default_ms = sieve_base_ms;
         rp.best_ns_per_prime = best_ms * per;
@@ -1780,11 +1800,11 @@ int mps_tune_save(const mps_ctx* c, const char* path) {
     if (!c || !path) return MPS_E_ARG;
     FILE* f = std::fopen(path, "w");
     if (!f) return MPS_E_ARG;
-    std::fprintf(f, "mps-tune 3\n");
+    std::fprintf(f, "mps-tune 4\n");
     for (const auto& kv : c->tuned)
-        std::fprintf(f, "%llu %u %u %u %u %u %u %.3f\n", (unsigned long long)kv.first, kv.second.cfg.kind,
+        std::fprintf(f, "%llu %u %u %u %u %u %u %u %u %.3f\n", (unsigned long long)kv.first, kv.second.cfg.kind,
                      kv.second.cfg.load_shift, kv.second.cfg.chains, kv.second.cfg.warps, kv.second.cfg.seg_words,
-                     kv.second.cfg.lanes, kv.second.ns_per_prime);
+                     kv.second.cfg.lanes, kv.second.cfg.fill, kv.second.cfg.scale, kv.second.ns_per_prime);
     return std::fclose(f) == 0 ? MPS_OK : MPS_E_ARG;
 }
 
@@ -1793,18 +1813,19 @@ int mps_tune_load(mps_ctx* c, const char* path) {
     FILE* f = std::fopen(path, "r");
     if (!f) return fail(c, MPS_E_ARG, std::string("cannot open ") + path);
     char head[32] = {0};
-    if (!std::fgets(head, sizeof(head), f) || std::strncmp(head, "mps-tune 3", 10) != 0) {
+    if (!std::fgets(head, sizeof(head), f) || std::strncmp(head, "mps-tune 4", 10) != 0) {
         std::fclose(f);
         return fail(c, MPS_E_ARG, "not a tuning file");
     }
     unsigned long long key;
-    unsigned kind, ls, ch, w, sw, lanes;
+    unsigned kind, ls, ch, w, sw, lanes, fill, scale;
     double ns;
-    while (std::fscanf(f, "%llu %u %u %u %u %u %u %lf", &key, &kind, &ls, &ch, &w, &sw, &lanes, &ns) == 8) {
+    while (std::fscanf(f, "%llu %u %u %u %u %u %u %u %u %lf", &key, &kind, &ls, &ch, &w, &sw, &lanes, &fill, &scale,
+                       &ns) == 10) {
         // only configurations the kernels are built for
         if (kind > 3 || ls < 1 || ls > 4 || (ch != 1 && ch != 2 && ch != 4) || w < 1 || w > 8 ||
             (sw != 1024 && sw != 2048 && sw != 4096) || (lanes != 32 && lanes != 16 && lanes != 8) ||
-            (lanes != 32 && (kind != 2 || ch == 4)))
+            (lanes != 32 && (kind != 2 || ch == 4)) || fill < 1 || fill > 256 || scale < 1 || scale > 1024)
             continue;
         TuneEntry te;
         te.cfg.kind = kind;
@@ -1813,6 +1834,8 @@ int mps_tune_load(mps_ctx* c, const char* path) {
         te.cfg.warps = w;
         te.cfg.seg_words = sw;
         te.cfg.lanes = lanes;
+        te.cfg.fill = fill;
+        te.cfg.scale = scale;
         te.ns_per_prime = ns;
         c->tuned[key] = te;
     }

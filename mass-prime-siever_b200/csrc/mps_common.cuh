@@ -25,6 +25,8 @@ constexpr u64 kFp64Limit = 1ull << 49;
 
 // Largest baby-step count of one prime (a table of 2^13 slots at load 1/2).
 constexpr u32 kMaxBaby = 4096;
+constexpr u32 kDefaultBabyScale = 256;   // m = ceil(sqrt(jcount)): equal baby and giant step counts
+constexpr u32 kDefaultFill = 192;        // fingerprint words: 3/4 of a key per word on average
 
 // Item constants, precomputed on the host once per item (all integer, exact).
 struct DevItem {
@@ -44,6 +46,7 @@ struct DevItem {
     u32 cmQ;               // cm mod Q
     u32 nsQ;               // n_start mod Q
     u32 max_baby;          // cap on the baby-step count m of this item (<= kMaxBaby)
+    u32 baby_scale;        // m = ceil(ceil(sqrt(jcount)) * baby_scale / 256) before the caps
     u32 item_index;
     u32 qf_n;              // prime factors of Q: qf_l[0..qf_n)
     u32 qf_l[7];

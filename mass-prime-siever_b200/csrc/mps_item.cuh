@@ -80,6 +80,7 @@ inline int item_constants(const mps_item* it, u32 class_modulus, u32 index, DevI
     d->cmQ = (u32)(cm % Q);
     d->nsQ = (u32)(d->n_start % Q);
     d->item_index = index;
+    d->baby_scale = kDefaultBabyScale;
     // the quadratic-character prefilter needs 0 < |b|, |c| < 2^32
     const unsigned __int128 lim = (unsigned __int128)1 << 32;
     if (babs > 0 && babs < lim && cabs > 0 && cabs < lim) {

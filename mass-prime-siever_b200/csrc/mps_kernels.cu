@@ -486,20 +486,16 @@ template <class F>
 __device__ void bsgs_setup(const F& f, u64 p, u64 b_mod, u64 t, const DevItem& it, u32 d, u32 r, const PrepArgs& a,
                            Counters* ctr) {
     typedef typename F::V V;
+    // the smallest k0 >= 0 with n_start + cm*k0 == r (mod d): k0*cmd == want
+    // (mod d) is solvable iff h = gcd(cmd, d) divides want, and then its
+    // solutions are k0 + per*i with per = d/h, k0 = (want/h)(cmd/h)^-1 mod per
     const u32 cmd = it.cmQ % d;                        // d | Q
     const u32 want = (r + d - it.nsQ % d) % d;
-    u32 k0 = 0, acc = 0;
-    bool ok = false;
-    for (; k0 < d; ++k0) {
-        if (acc == want) {
-            ok = true;
-            break;
-        }
-        acc += cmd;
-        if (acc >= d) acc -= d;
-    }
-    if (!ok || k0 >= it.K) return;
-    const u32 per = d / gcd32(d, cmd);                 // period of k
+    const u32 h = gcd32(cmd, d);                       // gcd(0, d) = d
+    if (want % h) return;
+    const u32 per = d / h;                             // period of k
+    const u32 k0 = (u32)((u64)(want / h) * inv_mod32((cmd / h) % per, per) % per);
+    if (k0 >= it.K) return;
     u64 jcount = ((u32)it.K - k0 + per - 1) / per;     // K < 2^32 (N1 - N0 <= 10^7)
     if (jcount > p) jcount = p;                        // ord(B) < p (Math.hpp:398-400)
     const u64 L = it.cm * per;
@@ -513,6 +509,7 @@ __device__ void bsgs_setup(const F& f, u64 p, u64 b_mod, u64 t, const DevItem& i
     if (jcount <= 1) return;
     const V Bv = f.pow(bv, L);
     u32 m = (u32)isqrt_ceil_dev(jcount);
+    if (it.baby_scale != 256) m = max(1u, (u32)(((u64)m * it.baby_scale + 255) >> 8));
     if (m > it.max_baby) m = it.max_baby;
     if (m > a.m_cap) m = a.m_cap;                      // never more than the launch's tables hold
     const u64 Bm = f.residue(f.pow(Bv, m));
@@ -1064,6 +1061,14 @@ __device__ u64 solve_fp64(const Entry& e, u32* tab, u32 tbits, u64* steps_out) {
 // and never walks inside the hot loop.
 
 constexpr u64 kQValid = 0x8000800080008000ull;
+
+// log2 of the words a prime with m baby steps gets: at least m * 256 / fill
+// words (fill 1..256; 0 counts as 256) and at least 32, at most 2^(tbits-1).
+__device__ __forceinline__ u32 fq_words_log(u32 m, u32 fill, u32 tbits, u32 extra_shift) {
+    const u32 f = fill - 1u < 256u ? fill : 256u;
+    const u32 need = (u32)(((u64)max(m, 2u) * 256u + f - 1) / f);
+    return min(tbits - 1, max(5u, 32u - __clz(need - 1) + extra_shift));
+}
 constexpr u32 kQOvf = 0x4000u;
 
 __device__ __forceinline__ u32 fq_pattern(u32 h, u32 tw) {
@@ -1117,14 +1122,14 @@ __device__ __forceinline__ bool fq_contains(const unsigned long long* tab, u32 m
 }
 
 template <int CH>
-__device__ u64 solve_fp64q(const Entry& e, unsigned long long* tab, u32 tbits, u64* steps_out) {
+__device__ u64 solve_fp64q(const Entry& e, unsigned long long* tab, u32 tbits, u32 fill, u64* steps_out) {
     const u32 lane = threadIdx.x & 31;
     Fp64 f;
     f.init(e.p);
     const u32 m = e.m;
     const u32 jc = (u32)e.jcount;                      // jcount <= 10^7
-    // 2^tw words for m keys (0.5..1 per word), within the launch's 2^(tbits-1) words
-    const u32 tw = min(tbits - 1, max(5u, 32u - __clz(max(m, 2u) - 1)));
+    // 2^tw words for m keys (at most fill/256 per word), within the launch's 2^(tbits-1) words
+    const u32 tw = fq_words_log(m, fill, tbits, 0);
     const u32 mask = (1u << tw) - 1, shift = 32 - tw;
     const double B = (double)e.B, Bm = (double)e.Bm, tv = (double)e.t, G0 = (double)e.G0;
 
@@ -1440,7 +1445,8 @@ __device__ __forceinline__ u32 xlow(const Fp64& f, double v, double two52) {   /
 __device__ __forceinline__ u32 xpattern(u32 lo) { return (((lo * kHashMul) >> 18) & 0x3FFFu) | 0x8000u; }
 
 template <int CH>
-__device__ u64 solve_fp64x(const Entry& e, unsigned long long* tab, u32 tbits, u32 load_shift, u64* steps_out) {
+__device__ u64 solve_fp64x(const Entry& e, unsigned long long* tab, u32 tbits, u32 load_shift, u32 fill,
+                           u64* steps_out) {
     const u32 lane = threadIdx.x & 31;
     const u32 word_shift = load_shift > 2 ? load_shift - 2 : 0;   // slot load 2^-load_shift, four slots a word
     const double two52 = 4503599627370496.0;
@@ -1449,7 +1455,7 @@ __device__ u64 solve_fp64x(const Entry& e, unsigned long long* tab, u32 tbits, u
     const u32 m = e.m;
     const u32 jc = (u32)e.jcount;                      // jcount <= 10^7
     // 2^tw words for m keys, within the launch's 2^(tbits-1) words (tw <= 16 keeps home and fingerprint apart)
-    const u32 tw = min(tbits - 1, max(5u, 32u - __clz(max(m, 2u) - 1) + word_shift));
+    const u32 tw = fq_words_log(m, fill, tbits, word_shift);
     const u32 mask = (1u << tw) - 1;
     const double B = (double)e.B, Bm = (double)e.Bm, tv = (double)e.t, G0 = (double)e.G0;
 
@@ -1573,11 +1579,11 @@ __device__ u64 solve_fp64x(const Entry& e, unsigned long long* tab, u32 tbits, u
 }
 
 template <int CH, int QT>
-__device__ __forceinline__ u64 solve_any(const Entry& e, void* tab, u32 tbits, u32 load_shift, u64* steps) {
+__device__ __forceinline__ u64 solve_any(const Entry& e, void* tab, u32 tbits, u32 load_shift, u32 fill, u64* steps) {
     if (CH == 0 || e.p >= kFp64Limit) return solve_entry<FieldM>(e, (unsigned short*)tab, tbits + 1, steps);
-    if (QT == 0) return solve_fp64q<CH ? CH : 1>(e, (unsigned long long*)tab, tbits, steps);
+    if (QT == 0) return solve_fp64q<CH ? CH : 1>(e, (unsigned long long*)tab, tbits, fill, steps);
     if (QT == 2) return solve_fp64h<CH ? CH : 1>(e, (unsigned short*)tab, tbits, load_shift, steps);
-    if (QT == 3) return solve_fp64x<CH ? CH : 1>(e, (unsigned long long*)tab, tbits, load_shift, steps);
+    if (QT == 3) return solve_fp64x<CH ? CH : 1>(e, (unsigned long long*)tab, tbits, load_shift, fill, steps);
     return solve_fp64<CH ? CH : 1>(e, (u32*)tab, tbits, steps);
 }
 
@@ -1601,18 +1607,39 @@ __global__ void __launch_bounds__(256, MPS_BSGS_MINB) k_bsgs(BsgsArgs a, Counter
     const u64 n_ent = min((u64)*(volatile unsigned long long*)&ctr->entries, a.ent_cap);
     u64 my_steps = 0;
     if (a.persistent) {
-        for (;;) {
-            u64 idx = 0;
-            if (lane == 0) idx = atomicAdd(&ctr->work_next, 1ull);
-            idx = __shfl_sync(FULL, idx, 0);
-            if (idx >= n_ent) break;
-            const Entry e = a.ent[idx];
+        // A warp claims the entry after the one it solves, and lanes 0..8 load
+        // that entry's nine words while the current one is solved, so neither
+        // the claim nor the load is waited for between entries.
+        static_assert(sizeof(Entry) == 72, "entry staging assumes nine 64-bit words");
+        u64 cur = 0;
+        if (lane == 0) cur = atomicAdd(&ctr->work_next, 1ull);
+        cur = __shfl_sync(FULL, cur, 0);
+        u64 claim = 0;                                          // lane 0: the entry after cur
+        if (lane == 0 && cur < n_ent) claim = atomicAdd(&ctr->work_next, 1ull);
+        u64 stage = cur < n_ent && lane < 9 ? reinterpret_cast<const u64*>(a.ent + cur)[lane] : 0;
+        while (cur < n_ent) {
+            Entry e;
+            e.p = __shfl_sync(FULL, stage, 0);
+            e.t = __shfl_sync(FULL, stage, 1);
+            e.G0 = __shfl_sync(FULL, stage, 2);
+            e.B = __shfl_sync(FULL, stage, 3);
+            e.Bm = __shfl_sync(FULL, stage, 4);
+            e.n_first = __shfl_sync(FULL, stage, 5);
+            e.L = __shfl_sync(FULL, stage, 6);
+            e.jcount = __shfl_sync(FULL, stage, 7);
+            const u64 w8 = __shfl_sync(FULL, stage, 8);
+            e.m = (u32)w8;                                      // little-endian: m, then item
+            e.item = (u32)(w8 >> 32);
+            const u64 next = __shfl_sync(FULL, claim, 0);
+            stage = next < n_ent && lane < 9 ? reinterpret_cast<const u64*>(a.ent + next)[lane] : 0;
+            if (lane == 0 && next < n_ent) claim = atomicAdd(&ctr->work_next, 1ull);
+            cur = next;
             if (!fits_table<CH, QT>(e, a.tbits)) {              // host sizing error: never overfill a table
                 if (lane == 0) atomicOr(&ctr->status, kStatusBadLaunch);
                 continue;
             }
             u64 steps = 0;
-            const u64 j = solve_any<CH, QT>(e, tab, a.tbits, a.load_shift, &steps);
+            const u64 j = solve_any<CH, QT>(e, tab, a.tbits, a.load_shift, a.fill, &steps);
             if (lane == 0) {
                 if (j != ~0ull) emit_relation(e.p, e.n_first + j * e.L, 0, e.item, a.rel, a.rel_cap, ctr);
                 my_steps += steps;
@@ -1628,7 +1655,7 @@ __global__ void __launch_bounds__(256, MPS_BSGS_MINB) k_bsgs(BsgsArgs a, Counter
             return;
         }
         u64 steps = 0;
-        const u64 j = solve_any<CH, QT>(e, tab, a.tbits, a.load_shift, &steps);
+        const u64 j = solve_any<CH, QT>(e, tab, a.tbits, a.load_shift, a.fill, &steps);
         if (lane == 0) {
             if (j != ~0ull) emit_relation(e.p, e.n_first + j * e.L, 0, e.item, a.rel, a.rel_cap, ctr);
             atomicAdd(&ctr->steps, (unsigned long long)steps);
@@ -2169,11 +2196,11 @@ __global__ void k_bsgs_direct(const u64* cases, u64* j_out, u64 count, u32 tbits
         M.init(p);
         const u64 rr = M.r2();
         e.Bm = M.from_mont(M.pow(M.to_mont(e.B, rr), m));
-        if (e.p >= kFp64Limit) result = solve_any<0, 0>(e, smem32, tbits, kDefaultLoadShift, nullptr);
-        else if (table_kind == 0) result = solve_any<2, 0>(e, smem32, tbits, kDefaultLoadShift, nullptr);
-        else if (table_kind == 2) result = solve_any<2, 2>(e, smem32, tbits, kDefaultLoadShift, nullptr);
-        else if (table_kind == 3) result = solve_any<2, 3>(e, smem32, tbits, 0, nullptr);
-        else result = solve_any<2, 1>(e, smem32, tbits, kDefaultLoadShift, nullptr);
+        if (e.p >= kFp64Limit) result = solve_any<0, 0>(e, smem32, tbits, kDefaultLoadShift, kDefaultFill, nullptr);
+        else if (table_kind == 0) result = solve_any<2, 0>(e, smem32, tbits, kDefaultLoadShift, kDefaultFill, nullptr);
+        else if (table_kind == 2) result = solve_any<2, 2>(e, smem32, tbits, kDefaultLoadShift, kDefaultFill, nullptr);
+        else if (table_kind == 3) result = solve_any<2, 3>(e, smem32, tbits, 0, kDefaultFill, nullptr);
+        else result = solve_any<2, 1>(e, smem32, tbits, kDefaultLoadShift, kDefaultFill, nullptr);
     }
     if (threadIdx.x == 0) j_out[idx] = result;
 }

@@ -102,6 +102,8 @@ struct BsgsArgs {
     u32 load_shift;            // table kind 2: at most 2^-load_shift of a prime's slots are used
     u32 lanes;                 // table kind 2: lanes per prime, 32 (a warp) or 16 / 8 (groups; every
                                // entry must have p < 2^49, max_p > 0 and < 2^49 or the caller's guarantee)
+    u32 fill;                  // table kinds 0 and 3: a prime's table has at least m * 256 / fill words
+                               // (1..256; 0 counts as 256), within the launch's 2^(tbits-1)
 };
 constexpr u32 kDefaultLoadShift = 2;
 cudaError_t launch_bsgs(const BsgsArgs& a, Counters* ctr, int grid, cudaStream_t s);

@@ -121,17 +121,20 @@ unsigned char* scratch_for_current_device(int* code) {
     return base;
 }
 
+// Keys the fingerprint words of a 4 << tb byte table hold at the default fill.
+u32 noalloc_holds(u32 tb) { return std::max<u32>(((1u << (tb - 1)) * kDefaultFill) >> 8, 1); }
+
 // The item's device constants with the default tuning: the split modulus
-// and the baby-step sizing of the regular entry points (fingerprint words, at
-// most one baby step per word on average, 2^11 words at most).
+// and the baby-step sizing of the regular entry points (fingerprint words at
+// the default fill, 2^11 words at most).
 int noalloc_item(const mps_item* it, DevItem* d, u32* tbits) {
     const char* why = "";
     if (int r = item_constants(it, 0, 0, d, &why)) return r;
     const u64 m_opt = (u64)std::ceil(std::sqrt((double)std::max<u64>(d->K, 1)));
     u32 tb = 6;
-    while ((1ull << (tb - 1)) < m_opt && tb < 11) ++tb;
+    while (noalloc_holds(tb) < m_opt && tb < 11) ++tb;
     *tbits = tb;
-    d->max_baby = std::min<u32>(1u << (tb - 1), kMaxBaby);
+    d->max_baby = std::min<u32>(noalloc_holds(tb), kMaxBaby);
     return MPS_OK;
 }
 
@@ -178,7 +181,7 @@ int run_pass(unsigned char* base, u64 lo, u64 hi, const DevItem& d, u32 tbits, i
     pa.ent_cap = kNoAllocEntries;
     pa.rel = rel;
     pa.rel_cap = kNoAllocRelations;
-    pa.m_cap = std::min<u32>(1u << (tbits - 1), kMaxBaby);   // fingerprint words: 2^(tbits-1) keys
+    pa.m_cap = std::min<u32>(noalloc_holds(tbits), kMaxBaby);
     BsgsArgs ba{};
     ba.ent = ent;
     ba.ent_cap = kNoAllocEntries;
@@ -190,6 +193,7 @@ int run_pass(unsigned char* base, u64 lo, u64 hi, const DevItem& d, u32 tbits, i
     ba.chains = 2;
     ba.table_kind = 0;
     ba.load_shift = kDefaultLoadShift;
+    ba.fill = kDefaultFill;
     ba.max_p = hi;
     OrderArgs oa{};
     oa.rel = rel;

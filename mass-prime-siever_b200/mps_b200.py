@@ -49,7 +49,8 @@ class Tuning(ctypes.Structure):
         ("bsgs_warps", ctypes.c_uint32), ("class_modulus", ctypes.c_uint32),
         ("full_mr", ctypes.c_uint32), ("plain", ctypes.c_uint32),
         ("chains", ctypes.c_uint32), ("graphs_off", ctypes.c_uint32), ("table_kind", ctypes.c_uint32),
-        ("load_shift", ctypes.c_uint32), ("lanes", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 2),
+        ("load_shift", ctypes.c_uint32), ("lanes", ctypes.c_uint32), ("table_fill", ctypes.c_uint32),
+        ("baby_scale", ctypes.c_uint32),
     ]
 
 
@@ -80,7 +81,8 @@ class TuneReport(ctypes.Structure):
     _fields_ = [("k_bits", ctypes.c_uint32), ("mod", ctypes.c_uint32), ("p_digits", ctypes.c_uint32),
                 ("candidates", ctypes.c_uint32), ("table_kind", ctypes.c_uint32), ("load_shift", ctypes.c_uint32),
                 ("chains", ctypes.c_uint32), ("warps", ctypes.c_uint32), ("seg_words", ctypes.c_uint32),
-                ("lanes", ctypes.c_uint32), ("best_ns_per_prime", ctypes.c_double),
+                ("lanes", ctypes.c_uint32), ("table_fill", ctypes.c_uint32), ("baby_scale", ctypes.c_uint32),
+                ("best_ns_per_prime", ctypes.c_double),
                 ("default_ns_per_prime", ctypes.c_double), ("sieve_best_ms", ctypes.c_double),
                 ("sieve_default_ms", ctypes.c_double), ("calib_bsgs_primes", ctypes.c_uint64)]
 

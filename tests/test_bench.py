@@ -43,10 +43,11 @@ def test_tuning_summary():
                  default_ns_per_prime=1.5),
             dict(table_kind=2, load_shift=2, chains=2, warps=4, seg_words=2048, lanes=32, best_ns_per_prime=2.0,
                  default_ns_per_prime=2.0),
-            dict(table_kind=0, load_shift=2, chains=4, warps=8, seg_words=4096, lanes=32, best_ns_per_prime=1.0,
-                 default_ns_per_prime=1.2)]
+            dict(table_kind=0, load_shift=2, chains=4, warps=8, seg_words=4096, lanes=32, table_fill=192,
+                 baby_scale=224, best_ns_per_prime=1.0, default_ns_per_prime=1.2)]
     s = bench.tuning_summary(reps, 3.0)
-    assert s["classes"] == 3 and s["choices"] == {"kind2/load2^-2/lanes32/ch2/w4/seg2048": 2, "kind0/ch4/w8/seg4096": 1}
+    assert s["classes"] == 3 and s["choices"] == {"kind2/load2^-2/lanes32/ch2/w4/seg2048": 2,
+                                                      "kind0/fill192/scale224/ch4/w8/seg4096": 1}
     assert s["bsgs_gain_vs_default"]["max"] == 1.5 and s["bsgs_gain_vs_default"]["min"] == 1.0
     assert bench.tuning_summary([], 0.0)["bsgs_gain_vs_default"] is None
 

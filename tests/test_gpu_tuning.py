@@ -17,7 +17,8 @@ def test_tuned_relations_equal_golden(mps_lib, golden, tmp_path):
         reports = s.autotune(items)
         assert reports and all(r["candidates"] >= 10 for r in reports)
         for r in reports:
-            assert r["table_kind"] in (0, 2) and r["chains"] in (1, 2, 4) and r["warps"] in (4, 8)
+            assert r["table_kind"] in (0, 2, 3) and r["chains"] in (1, 2, 4) and r["warps"] in (4, 8)
+            assert 1 <= r["table_fill"] <= 256 and 1 <= r["baby_scale"] <= 1024
             assert r["best_ns_per_prime"] <= r["default_ns_per_prime"] * 1.0001
             assert r["seg_words"] in (1024, 2048, 4096) and r["lanes"] in (8, 16, 32)
         for c, it in zip(cases, items):
@@ -28,7 +29,7 @@ def test_tuned_relations_equal_golden(mps_lib, golden, tmp_path):
         path = str(tmp_path / "tune.txt")
         s.tune_save(path)
     text = open(path).read().splitlines()
-    assert text[0] == "mps-tune 3" and len(text) == 1 + len(reports)
+    assert text[0] == "mps-tune 4" and len(text) == 1 + len(reports)
     with mps_lib.Siever(0) as s2:
         s2.tune_load(path)
         for c, it in zip(cases, items):
@@ -38,9 +39,10 @@ def test_tuned_relations_equal_golden(mps_lib, golden, tmp_path):
 
 def test_tuning_file_with_bad_lines(mps_lib, tmp_path, golden):
     path = tmp_path / "tune.txt"
-    # a kind, chain count and warp count the kernels are not built for are skipped
-    path.write_text("mps-tune 3\n1 9 2 2 4 2048 32 1.0\n2 2 2 3 4 2048 32 1.0\n3 2 2 2 99 2048 32 1.0\n"
-                    "4 2 2 2 4 3000 32 1.0\n5 0 2 2 4 2048 8 1.0\n6 2 2 4 4 2048 16 1.0\n")
+    # a kind, chain count, warp count, segment, lane split, fill or scale the kernels are not built for is skipped
+    path.write_text("mps-tune 4\n1 9 2 2 4 2048 32 192 256 1.0\n2 2 2 3 4 2048 32 192 256 1.0\n"
+                    "3 2 2 2 99 2048 32 192 256 1.0\n4 2 2 2 4 3000 32 192 256 1.0\n5 0 2 2 4 2048 8 192 256 1.0\n"
+                    "6 2 2 4 4 2048 16 192 256 1.0\n7 0 2 2 4 2048 32 0 256 1.0\n8 3 2 2 4 2048 32 192 2000 1.0\n")
     case = next(c for c in golden["cases"] if c["name"] == "selftest")
     with mps_lib.Siever(0) as s:
         s.tune_load(str(path))
