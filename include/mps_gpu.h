@@ -65,8 +65,9 @@ typedef struct mps_tuning {
     uint64_t chunk_odds;        /* odd integers per device chunk (0: 2^26)                      */
     uint32_t max_baby;          /* cap on the baby-step count (0: what the table holds)        */
     uint32_t bsgs_warps;        /* warps per BSGS block (0: 4)                                 */
-    uint32_t class_modulus;     /* Q of the power-residue split g = gcd(Q, p-1)
-                                   (0: lcm(mod, 5040), or 5040 when that exceeds 100800;
+    uint32_t class_modulus;     /* Q of the power-residue split g = gcd(Q, p-1), even, <= 2^28
+                                   (0: lcm(mod, 720720), else lcm(mod, 5040), whichever first
+                                    stays within 2^28, else 5040;
                                     1: lcm(mod, 2), the reference's plain-method filter)       */
     uint32_t full_mr;           /* 1: 12-base Miller-Rabin on every filter survivor (eager)    */
     uint32_t plain;             /* 1: plain per-chunk path (host sync between stages)          */

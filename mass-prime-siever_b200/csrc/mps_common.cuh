@@ -49,7 +49,7 @@ struct DevItem {
     u32 baby_scale;        // m = ceil(ceil(sqrt(jcount)) * baby_scale / 256) before the caps
     u32 item_index;
     u32 qf_n;              // prime factors of Q: qf_l[0..qf_n)
-    u32 qf_l[7];
+    u32 qf_l[9];
     // Quadratic-character prefilter (both |b| and |c| below 2^32): for x = b
     // and x = -c, x = (-1)^neg 2^k o with o odd; rcp = floor((2^64-1) / o).
     u32 qr_on;

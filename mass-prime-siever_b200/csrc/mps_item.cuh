@@ -20,14 +20,23 @@ inline u64 gcd_host(u64 a, u64 b) {
     return a;
 }
 
-// The split modulus Q of a tuning value: 0 -> lcm(cm, 5040) (5040 when that
-// exceeds 100800); 1 -> lcm(cm, 2), the reference's plain-method filter
-// (Gpu.hpp:247-298: the Legendre test and the gcd(mod, p-1)-th power test);
-// anything else as given.
+constexpr u64 kMaxSplit = 1ull << 28;       // largest split modulus (at most 9 distinct primes)
+
+// The split modulus Q of a tuning value: 0 -> lcm(cm, B) for the first B of
+// kSplitBases whose lcm stays within 2^28 (5040 when none does); 1 ->
+// lcm(cm, 2), the reference's plain-method filter (Gpu.hpp:247-298: the
+// Legendre test and the gcd(mod, p-1)-th power test); anything else as given.
+// Every prime l of Q with l | p - 1 splits a prime's exponents into l classes
+// and keeps one, so a larger Q leaves fewer BSGS steps (about 1/(l-1) of the
+// primes gain a factor l); the prep pays a longer walk for them.
+constexpr u64 kSplitBases[] = {720720ull, 5040ull};   // 2^4 3^2 5 7 11 13, 2^4 3^2 5 7
 inline u64 split_modulus(u32 class_modulus, u64 cm) {
     if (class_modulus == 0) {
-        const u64 l = cm / gcd_host(cm, 5040) * 5040;
-        return l <= 100800 ? l : 5040;
+        for (u64 base : kSplitBases) {
+            const u64 l = cm / gcd_host(cm, base) * base;
+            if (l <= kMaxSplit) return l;
+        }
+        return 5040;
     }
     if (class_modulus == 1) return cm % 2 == 0 ? cm : 2 * cm;
     return class_modulus;
@@ -66,8 +75,8 @@ inline int item_constants(const mps_item* it, u32 class_modulus, u32 index, DevI
     d->has_work = (it->N1 > 0 && d->n_start < d->N1) ? 1 : 0;
     d->K = d->has_work ? (d->N1 - d->n_start + cm - 1) / cm : 0;
     const u64 Q = split_modulus(class_modulus, cm);
-    // Q < 2^20 has at most 7 distinct prime factors (2*3*5*7*11*13*17*19 > 2^20)
-    if (Q < 2 || Q > (1u << 20) || (Q & 1)) return *why = "class_modulus must be even and <= 2^20", MPS_E_ARG;
+    // Q <= 2^28 has at most 9 distinct prime factors (2*3*5*...*29 > 2^28)
+    if (Q < 2 || Q > kMaxSplit || (Q & 1)) return *why = "class_modulus must be even and <= 2^28", MPS_E_ARG;
     d->Q = (u32)Q;
     d->Q_rcp = ~0ull / Q;
     u64 x = Q;

@@ -472,7 +472,7 @@ __device__ bool power_split_pp(const F& f, u64 p, u64 b_mod, u64 t, const DevIte
         }
         if (!found) return false;
         // r' == r (mod d), r' == xr (mod dl); d, dl coprime
-        u32 step = 0;                                      // d * dl <= g <= Q < 2^21
+        u32 step = 0;                                      // d * dl <= g <= Q <= 2^28
         while ((r + d * step) % dl != xr) ++step;
         r += d * step;
         d *= dl;
@@ -1426,23 +1426,25 @@ __device__ u64 solve_fp64h(const Entry& e, unsigned short* tab, u32 tbits, u32 l
 //
 // The table of solve_fp64q (four 16-bit fingerprints per 64-bit word, bit 15
 // of a half marks it used, bit 14 of half 0 is the word's overflow bit), with
-// the key taken from the canonical residue itself: x + 2^52 (one FP64 add)
-// holds x in its low mantissa bits, so the low 32 bits of x come out of the
-// register for free.  The home word is the low tw bits of x (a residue spread
-// over [0, p)), the fingerprint 14 high bits of a multiplicative hash.  The
-// next giant value is multiplied before the probe of the current one, so the
-// multiply's latency overlaps the shared-memory load and the vote.  A word
-// holds at most 2^-word_shift keys on average (word_shift 0: one key per word).
+// the key taken from the canonical residue's integer: x + 2^52 (one FP64 add)
+// holds x in its low 52 bits, and a multiplicative hash of its two 32-bit
+// words gives the home word (the top bits) and the 14-bit fingerprint (the
+// bits below them), as in solve_fp64q.  Hashing both words matters: residues
+// that are small multiples of powers of two (t * 2^(L i) before the first
+// reduction, b = 2) share their low bits and would pile into one home word.
+// The next giant value is multiplied before the probe of the current one, so
+// the multiply's latency overlaps the shared-memory load and the vote.  A
+// word holds at most 2^-word_shift of the fill on average.
 
-__device__ __forceinline__ u32 xlow(const Fp64& f, double v, double two52) {   // low 32 bits of canon(v)
-    double u = __dadd_rn(v, two52);
-    if (v < 0.0) u = __dadd_rn(u, f.p);
-    return (u32)__double2loint(u);
+__device__ __forceinline__ u32 xhash_bits(double u) {           // u = x + 2^52, x canonical
+    return (u32)(__double2loint(u) ^ __double2hiint(u)) * kHashMul;
 }
 
-// The fingerprint: bits 18..31 of lo * an odd constant (an integer multiply-add,
-// which runs on the FMA pipe), so that residues below 2^32 still spread.
-__device__ __forceinline__ u32 xpattern(u32 lo) { return (((lo * kHashMul) >> 18) & 0x3FFFu) | 0x8000u; }
+__device__ __forceinline__ u32 xhash(const Fp64& f, double v, double two52) {   // hash of canon(v)
+    double u = __dadd_rn(v, two52);
+    if (v < 0.0) u = __dadd_rn(u, f.p);
+    return xhash_bits(u);
+}
 
 template <int CH>
 __device__ u64 solve_fp64x(const Entry& e, unsigned long long* tab, u32 tbits, u32 load_shift, u32 fill,
@@ -1454,9 +1456,9 @@ __device__ u64 solve_fp64x(const Entry& e, unsigned long long* tab, u32 tbits, u
     f.init(e.p);
     const u32 m = e.m;
     const u32 jc = (u32)e.jcount;                      // jcount <= 10^7
-    // 2^tw words for m keys, within the launch's 2^(tbits-1) words (tw <= 16 keeps home and fingerprint apart)
+    // 2^tw words for m keys, within the launch's 2^(tbits-1) words
     const u32 tw = fq_words_log(m, fill, tbits, word_shift);
-    const u32 mask = (1u << tw) - 1;
+    const u32 mask = (1u << tw) - 1, shift = 32 - tw;
     const double B = (double)e.B, Bm = (double)e.Bm, tv = (double)e.t, G0 = (double)e.G0;
 
     double xb = B, xg = Bm;                            // B^(l+1), Bm^(l+1)
@@ -1509,8 +1511,8 @@ __device__ u64 solve_fp64x(const Entry& e, unsigned long long* tab, u32 tbits, u
         for (int c = 0; c < CH; ++c) {
             const u32 i = base + 32 * c + lane;
             if (i < lim) {
-                const u32 lo = (u32)__double2loint(__dadd_rn(cv[c], two52));
-                fq_insert(tab, mask, lo & mask, xpattern(lo));
+                const u32 h = xhash_bits(__dadd_rn(cv[c], two52));
+                fq_insert(tab, mask, h >> shift, fq_pattern(h, tw));
             }
         }
         if (cb) {
@@ -1533,22 +1535,22 @@ __device__ u64 solve_fp64x(const Entry& e, unsigned long long* tab, u32 tbits, u
         giant_done = G;
         const uint2* t2 = reinterpret_cast<const uint2*>(tab);
         for (u32 base = 0; base < G; base += 32 * CH) {
-            u32 los[CH];
+            u32 hs[CH];
             double nx[CH];
             u32 cand = 0;
 #pragma unroll
             for (int c = 0; c < CH; ++c) {
-                los[c] = xlow(f, gx[c], two52);
+                hs[c] = xhash(f, gx[c], two52);
                 nx[c] = f.mul(gx[c], Gstep);              // the next value, independent of the probe
-                const uint2 w = t2[los[c] & mask];
-                cand |= fq_candidate(w.x, w.y, xpattern(los[c])) ? (1u << c) : 0u;
+                const uint2 w = t2[hs[c] >> shift];
+                cand |= fq_candidate(w.x, w.y, fq_pattern(hs[c], tw)) ? (1u << c) : 0u;
             }
             if (__any_sync(FULL, cand)) {
                 u32 real = 0;
 #pragma unroll
                 for (int c = 0; c < CH; ++c)
                     if (((cand >> c) & 1u) && base + 32 * c + lane + 1 <= G &&
-                        fq_contains(tab, mask, los[c] & mask, xpattern(los[c])))
+                        fq_contains(tab, mask, hs[c] >> shift, fq_pattern(hs[c], tw)))
                         real |= 1u << c;
                 u64 jb = ~0ull;
 #pragma unroll
