@@ -270,12 +270,13 @@ def kernel_rooflines(siever, pieces, peaks, fp64_path: bool) -> dict:
     independent-chain mulmod rate of the same arithmetic without table work.
     k_sieve: achieved = algorithmic bit-marks (sum of 1/q per odd) per second;
     peak = the live-measured conflict-free shared-memory atomicOr rate."""
-    tot = {"steps": 0, "odds": 0, "marks": 0.0, "entries": 0, "survivors": 0,
+    tot = {"steps": 0, "baby": 0, "odds": 0, "marks": 0.0, "entries": 0, "survivors": 0,
            "bsgs_ms": 0.0, "sieve_ms": 0.0, "prep_ms": 0.0, "order_ms": 0.0, "launches": 0}
     for lo, hi, item in pieces:
         siever.chunk_relations(lo, hi, item)
         st = siever.stats()
         tot["steps"] += st["bsgs_steps"]
+        tot["baby"] += st.get("bsgs_baby_steps", 0)
         tot["odds"] += st["odds"]
         tot["marks"] += st["odds"] * sieve_marks_per_odd(hi)
         tot["entries"] += st["entries"]
@@ -293,6 +294,7 @@ def kernel_rooflines(siever, pieces, peaks, fp64_path: bool) -> dict:
             "kernel": "k_bsgs", "achieved": rate / 1e9, "peak": mul_peak / 1e9, "unit": "G mulmod/s",
             "frac": rate / mul_peak if mul_peak else None, "peak_kind": "of measured (live probe)",
             "avg_launch_ms": tot["bsgs_ms"] / n, "steps_per_launch": tot["steps"] / n,
+            "baby_steps_per_launch": tot["baby"] / n, "entries_per_launch": tot["entries"] / n,
             "traffic": traffic * tot["steps"] / n if traffic is not None else None,
             "traffic_unit": "DRAM bytes per launch", "traffic_source": traffic_src,
             "hbm_side": {"algorithmic_bytes_per_launch": 72.0 * tot["entries"] / n,

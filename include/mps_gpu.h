@@ -102,6 +102,7 @@ typedef struct mps_stats {
     double   sieve_ms;          /* device time of the sieve kernel (CUDA events)  */
     double   prep_ms;           /* device time of the prep kernel                 */
     double   order_ms;          /* device time of the order kernel                */
+    uint64_t bsgs_baby_steps;   /* the baby steps among bsgs_steps                */
 } mps_stats;
 
 /* ---- context (replaces CudaSiever::init, Cuda.hpp:198-257) ---- */

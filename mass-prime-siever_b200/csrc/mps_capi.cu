@@ -475,6 +475,7 @@ int run_chunk(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, const LaunchCfg& g_it
     }
     c->stats.odds += n_odds;
     c->stats.bsgs_steps += h.steps;
+    c->stats.bsgs_baby_steps += h.baby;
     c->stats.survivors += h.survivors;
     c->stats.entries += h.entries;
     c->stats.chunks += 1;
@@ -694,6 +695,7 @@ int slot_finish(mps_ctx* c, WaveSlot& w, std::vector<RawRelation>& out) {
     for (u64 i = 0; i < nr; ++i)
         if (w.h_rel[i].q != ~0ull) out.push_back(w.h_rel[i]);
     c->stats.bsgs_steps += h.steps;
+    c->stats.bsgs_baby_steps += h.baby;
     c->stats.survivors += h.survivors;
     c->stats.entries += h.entries;
     c->stats.chunks += 1;

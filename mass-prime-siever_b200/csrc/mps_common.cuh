@@ -89,6 +89,7 @@ struct Counters {
     unsigned long long primes;     u64 pad5[7];   // prime count (counting kernel only)
     unsigned long long steps;      u64 pad6[7];   // baby + giant steps executed by the BSGS
     unsigned long long prep_next;  u64 pad7[7];   // next survivor the prep's warps claim
+    unsigned long long baby;       u64 pad8[7];   // the baby steps among `steps`
 };
 
 // Status bits a kernel may set (host turns them into error codes).

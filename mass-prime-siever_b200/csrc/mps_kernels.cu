@@ -758,6 +758,10 @@ __device__ __noinline__ int find_baby_index(const F& f, typename F::V tbl, typen
     return -1;
 }
 
+// A solve's step counts for its caller: giant steps in the high 32 bits,
+// baby steps in the low 32 (baby <= kMaxBaby, giant <= jcount <= 10^7).
+__device__ __forceinline__ u64 pack_steps(u64 baby, u64 giant) { return (giant << 32) | baby; }
+
 // Solves one entry with the 32 lanes of the calling warp; returns the
 // smallest j (< jcount) or ~0ull.  Two interleaved chains per lane: baby
 // indices i = l + 64k and l + 32 + 64k, giant steps g = 1 + l + 64k and
@@ -797,7 +801,7 @@ __device__ u64 solve_entry(const Entry& e, unsigned short* tab, u32 tbits, u64* 
 
     // baby steps t*B^i, stopping at a cycle B^d == 1 (d < m)
     u32 cyc = 0;
-    u64 steps = 0;
+    u64 steps = 0, baby_steps = 0;
     for (u32 base = 0; base < m; base += 64) {
         const u32 i0 = base + lane, i1 = base + 32 + lane;
         const u64 k0 = f.key(f.canon(baby0)), k1 = f.key(f.canon(baby1));
@@ -811,6 +815,7 @@ __device__ u64 solve_entry(const Entry& e, unsigned short* tab, u32 tbits, u64* 
         if (i0 < lim) table_insert(tab, mask, tbits, k0);
         if (i1 < lim) table_insert(tab, mask, tbits, k1);
         steps += min(64u, lim - base);
+        baby_steps += min(64u, lim - base);
         if (cyc) break;
         baby0 = f.mul(baby0, B64);
         baby1 = f.mul(baby1, B64);
@@ -856,7 +861,7 @@ __device__ u64 solve_entry(const Entry& e, unsigned short* tab, u32 tbits, u64* 
         }
     }
     __syncwarp();
-    if (steps_out) *steps_out = steps;
+    if (steps_out) *steps_out = pack_steps(baby_steps, steps - baby_steps);
     return best < e.jcount ? best : ~0ull;
 }
 
@@ -1038,7 +1043,7 @@ __device__ u64 solve_fp64(const Entry& e, u32* tab, u32 tbits, u64* steps_out) {
         }
     }
     __syncwarp();
-    if (steps_out) *steps_out = (u64)baby_done + giant_done;
+    if (steps_out) *steps_out = pack_steps(baby_done, giant_done);
     return best < e.jcount ? best : ~0ull;
 }
 
@@ -1248,7 +1253,7 @@ __device__ u64 solve_fp64q(const Entry& e, unsigned long long* tab, u32 tbits, u
         }
     }
     __syncwarp();
-    if (steps_out) *steps_out = (u64)baby_done + giant_done;
+    if (steps_out) *steps_out = pack_steps(baby_done, giant_done);
     return best < e.jcount ? best : ~0ull;
 }
 
@@ -1418,7 +1423,7 @@ __device__ u64 solve_fp64h(const Entry& e, unsigned short* tab, u32 tbits, u32 l
         }
     }
     __syncwarp();
-    if (steps_out) *steps_out = (u64)baby_done + giant_done;
+    if (steps_out) *steps_out = pack_steps(baby_done, giant_done);
     return best < e.jcount ? best : ~0ull;
 }
 
@@ -1576,7 +1581,7 @@ __device__ u64 solve_fp64x(const Entry& e, unsigned long long* tab, u32 tbits, u
         }
     }
     __syncwarp();
-    if (steps_out) *steps_out = (u64)baby_done + giant_done;
+    if (steps_out) *steps_out = pack_steps(baby_done, giant_done);
     return best < e.jcount ? best : ~0ull;
 }
 
@@ -1607,7 +1612,7 @@ __global__ void __launch_bounds__(256, MPS_BSGS_MINB) k_bsgs(BsgsArgs a, Counter
     const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     u32* tab = smem32 + (size_t)warp * (1u << a.tbits);
     const u64 n_ent = min((u64)*(volatile unsigned long long*)&ctr->entries, a.ent_cap);
-    u64 my_steps = 0;
+    u64 my_steps = 0, my_baby = 0;
     if (a.persistent) {
         // A warp claims the entry after the one it solves, and lanes 0..8 load
         // that entry's nine words while the current one is solved, so neither
@@ -1644,10 +1649,14 @@ __global__ void __launch_bounds__(256, MPS_BSGS_MINB) k_bsgs(BsgsArgs a, Counter
             const u64 j = solve_any<CH, QT>(e, tab, a.tbits, a.load_shift, a.fill, &steps);
             if (lane == 0) {
                 if (j != ~0ull) emit_relation(e.p, e.n_first + j * e.L, 0, e.item, a.rel, a.rel_cap, ctr);
-                my_steps += steps;
+                my_steps += (steps & 0xFFFFFFFFull) + (steps >> 32);
+                my_baby += steps & 0xFFFFFFFFull;
             }
         }
-        if (lane == 0 && my_steps) atomicAdd(&ctr->steps, (unsigned long long)my_steps);
+        if (lane == 0 && my_steps) {
+            atomicAdd(&ctr->steps, (unsigned long long)my_steps);
+            atomicAdd(&ctr->baby, (unsigned long long)my_baby);
+        }
     } else {
         const u64 idx = (u64)blockIdx.x * a.warps_per_block + warp;
         if (idx >= n_ent) return;
@@ -1660,7 +1669,8 @@ __global__ void __launch_bounds__(256, MPS_BSGS_MINB) k_bsgs(BsgsArgs a, Counter
         const u64 j = solve_any<CH, QT>(e, tab, a.tbits, a.load_shift, a.fill, &steps);
         if (lane == 0) {
             if (j != ~0ull) emit_relation(e.p, e.n_first + j * e.L, 0, e.item, a.rel, a.rel_cap, ctr);
-            atomicAdd(&ctr->steps, (unsigned long long)steps);
+            atomicAdd(&ctr->steps, (unsigned long long)((steps & 0xFFFFFFFFull) + (steps >> 32)));
+            atomicAdd(&ctr->baby, (unsigned long long)(steps & 0xFFFFFFFFull));
         }
     }
 }
@@ -1707,7 +1717,7 @@ __global__ void __launch_bounds__(256, MPS_BSGS_MINB) k_bsgs_groups(BsgsArgs a, 
                           (size_t)grp * group_slots;
     const u32 tw_max = a.tbits + 1 - NG_LOG;
     const u64 n_ent = min((u64)*(volatile unsigned long long*)&ctr->entries, a.ent_cap);
-    u64 my_steps = 0;
+    u64 my_steps = 0, my_baby = 0;
     for (;;) {
         u64 first = 0;
         if (lane == 0) first = atomicAdd(&ctr->work_next, (unsigned long long)NG);
@@ -1845,9 +1855,13 @@ __global__ void __launch_bounds__(256, MPS_BSGS_MINB) k_bsgs_groups(BsgsArgs a, 
         if (gl == 0 && active) {
             if (best < e.jcount) emit_relation(e.p, e.n_first + best * e.L, 0, e.item, a.rel, a.rel_cap, ctr);
             my_steps += (u64)baby_done + giant_done;
+            my_baby += baby_done;
         }
     }
-    if (gl == 0 && my_steps) atomicAdd(&ctr->steps, (unsigned long long)my_steps);
+    if (gl == 0 && my_steps) {
+        atomicAdd(&ctr->steps, (unsigned long long)my_steps);
+        atomicAdd(&ctr->baby, (unsigned long long)my_baby);
+    }
 }
 
 // -------------------------------------------------------------- the order --

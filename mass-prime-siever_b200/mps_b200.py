@@ -60,7 +60,7 @@ class Stats(ctypes.Structure):
         ("relations", ctypes.c_uint64), ("chunks", ctypes.c_uint64), ("device_ms", ctypes.c_double),
         ("bsgs_ms", ctypes.c_double), ("bsgs_launches", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint64),
         ("bsgs_steps", ctypes.c_uint64), ("sieve_ms", ctypes.c_double), ("prep_ms", ctypes.c_double),
-        ("order_ms", ctypes.c_double),
+        ("order_ms", ctypes.c_double), ("bsgs_baby_steps", ctypes.c_uint64),
     ]
 
 
