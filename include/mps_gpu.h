@@ -66,8 +66,8 @@ typedef struct mps_tuning {
     uint32_t max_baby;          /* cap on the baby-step count (0: what the table holds)        */
     uint32_t bsgs_warps;        /* warps per BSGS block (0: 4)                                 */
     uint32_t class_modulus;     /* Q of the power-residue split g = gcd(Q, p-1), even, <= 2^28
-                                   (0: lcm(mod, 720720), else lcm(mod, 5040), whichever first
-                                    stays within 2^28, else 5040;
+                                   (0: lcm(mod, 232792560), else lcm(mod, 720720), else
+                                    lcm(mod, 5040), the first within 2^28, else 5040;
                                     1: lcm(mod, 2), the reference's plain-method filter)       */
     uint32_t full_mr;           /* 1: 12-base Miller-Rabin on every filter survivor (eager)    */
     uint32_t plain;             /* 1: plain per-chunk path (host sync between stages)          */
@@ -76,15 +76,16 @@ typedef struct mps_tuning {
     uint32_t table_kind;        /* BSGS table: 0 = four 16-bit fingerprints per 64-bit word,
                                    1 = one 32-bit key per slot, 2 = one 16-bit fingerprint
                                    per slot, read with one 16-bit load per probe, 3 = the
-                                   words of 0 keyed from the FP64 pipe (no integer hash)       */
-    uint32_t load_shift;        /* table kinds 2 and 3: a prime's table has at least
-                                   2^load_shift slots per baby step (0: 2)                      */
+                                   words of 0 filled by warp-cooperative stores (a
+                                   compare-and-swap only when a word is full)               */
+    uint32_t load_shift;        /* table kind 2: a prime's table has at least 2^load_shift
+                                   slots per baby step (0: 2)                                   */
     uint32_t lanes;             /* table kind 2: lanes per prime, 32, 16 or 8 (0: 32); groups of
                                    16 or 8 solve 2 or 4 primes per warp, for p < 2^49          */
     uint32_t table_fill;        /* table kinds 0 and 3: at most table_fill/256 keys per 64-bit
-                                   word on average, 1..256 (0: 192)                            */
+                                   word on average, 1..256 (0: 160)                            */
     uint32_t baby_scale;        /* baby steps m = ceil(sqrt(j range) * baby_scale / 256) before
-                                   the table's cap, 1..1024 (0: 256, the square root)          */
+                                   the table's cap, 1..1024 (0: 160; 256 is the square root)   */
 } mps_tuning;
 
 /* Counters of the last call (all chunks of it). */

@@ -249,7 +249,7 @@ u32 table_holds(const LaunchCfg& g, u32 tb) {
     const u32 fill = g.fill - 1 < 256 ? g.fill : 256;
     if (g.kind == 0) return std::max<u32>(((1u << (tb - 1)) * fill) >> 8, 1);
     if (g.kind == 2) return std::max<u32>(1u << (tb + 1 - g.load_shift) >> groups_log(g), 1);
-    if (g.kind == 3) return std::max<u32>(((1u << (tb + 1 - std::max<u32>(g.load_shift, 2))) * fill) >> 8, 1);
+    if (g.kind == 3) return std::max<u32>(((1u << (tb - 1)) * fill) >> 8, 1);      // the words of kind 0
     return std::max<u32>((1u << tb) / 5, 1);
 }
 
@@ -263,16 +263,18 @@ u32 table_room(const LaunchCfg& g, u32 tb) {
 
 // Baby-step table size for an item: 4 << tbits bytes per warp, at most
 // 8 KB by default (keeps ~24 warps resident per SM).  Every prime's j-range
-// is at most K, so m_opt = ceil(sqrt(K)) baby steps balance the giant steps;
-// a wider N range than the table holds trades baby steps for giant steps.
-// Fingerprint table (table_kind 0): 2^(tbits-1) words of four keys, filled
-// to at most one key per word on average.  32-bit slots (table_kind 1):
-// 2^tbits slots, load at most 1/5 (a probe then reads one slot).  16-bit
-// slots (table_kind 2): 2^(tbits+1) slots, a prime's keys at most
-// 2^-load_shift of them (up to 12 bits, 16 KB per warp, when load_shift > 2).
+// is at most K, so m_opt = ceil(sqrt(K)) x scale/256 baby steps is the most a
+// prime of the item asks for; a wider N range than the table holds trades
+// baby steps for giant steps.  Fingerprint words (table kinds 0 and 3):
+// 2^(tbits-1) words of four keys, filled to at most fill/256 keys per word on
+// average.  32-bit slots (table_kind 1): 2^tbits slots, load at most 1/5 (a
+// probe then reads one slot).  16-bit slots (table_kind 2): 2^(tbits+1)
+// slots, a prime's keys at most 2^-load_shift of them (up to 12 bits, 16 KB
+// per warp, when load_shift > 2).
 void table_for(const mps_ctx* c, const LaunchCfg& g, u64 K, u32* tbits, u32* max_baby) {
-    const u64 m_opt = (u64)std::ceil(std::sqrt((double)std::max<u64>(K, 1)));
-    const u32 top = (g.kind == 2 || g.kind == 3) && g.load_shift > 2 ? 12 : 11;
+    const u64 m_sqrt = (u64)std::ceil(std::sqrt((double)std::max<u64>(K, 1)));
+    const u64 m_opt = std::max<u64>(1, (m_sqrt * g.scale + 255) / 256);
+    const u32 top = g.kind == 2 && g.load_shift > 2 ? 12 : 11;
     u32 tb = c->tun.table_bits;
     if (tb == 0) {
         tb = 6;
@@ -1664,18 +1666,14 @@ int mps_autotune(mps_ctx* c, const mps_item* items, size_t n_items, mps_tune_rep
     const LaunchCfg base = default_cfg(c);
     std::vector<LaunchCfg> cands{base};
     for (u32 kind : {0u, 3u})
-        for (u32 ls : {2u, 3u}) {
-            if (kind == 0 && ls != 2) continue;
-            for (u32 ch : {1u, 2u, 4u})
-                for (u32 w : {4u, 8u}) {
-                    LaunchCfg g;
-                    g.kind = kind;
-                    g.load_shift = kind == 3 ? ls : base.load_shift;
-                    g.chains = ch;
-                    g.warps = w;
-                    if (g != base) cands.push_back(g);
-                }
-        }
+        for (u32 ch : {1u, 2u, 4u})
+            for (u32 w : {4u, 8u}) {
+                LaunchCfg g;
+                g.kind = kind;
+                g.chains = ch;
+                g.warps = w;
+                if (g != base) cands.push_back(g);
+            }
     // lanes per prime: groups of 16 or 8 lanes (table kind 2, 1 or 2 chains)
     for (u32 lanes : {16u, 8u})
         for (u32 ch : {1u, 2u})
@@ -1704,8 +1702,8 @@ int mps_autotune(mps_ctx* c, const mps_item* items, size_t n_items, mps_tune_rep
         // phase 1: the BSGS configuration by the BSGS kernel's time; phase 2: with
         // it, the table fill and the baby-step scale (fingerprint words only);
         // phase 3: the sieve's segment size by the sieve kernel's time
-        constexpr u32 kFills[] = {256u, 224u, 192u, 160u, 128u};
-        constexpr u32 kScales[] = {256u, 224u, 192u, 160u};
+        constexpr u32 kFills[] = {224u, 192u, 160u, 128u};
+        constexpr u32 kScales[] = {224u, 192u, 160u, 128u};
         const size_t n_bsgs = cands.size();
         const size_t n_fill = n_bsgs + (sizeof(kFills) / sizeof(kFills[0])) * (sizeof(kScales) / sizeof(kScales[0]));
         const size_t n_all = n_fill + 3;

@@ -25,8 +25,11 @@ constexpr u64 kFp64Limit = 1ull << 49;
 
 // Largest baby-step count of one prime (a table of 2^13 slots at load 1/2).
 constexpr u32 kMaxBaby = 4096;
-constexpr u32 kDefaultBabyScale = 256;   // m = ceil(sqrt(jcount)): equal baby and giant step counts
-constexpr u32 kDefaultFill = 192;        // fingerprint words: 3/4 of a key per word on average
+// Measured on the B200 (C2 and C3 slices): a baby step (hash, insert) costs
+// about twice a giant step (hash, probe), so m = 0.625 sqrt(jcount) beats the
+// square root, and words filled to 0.625 keys overflow rarely enough.
+constexpr u32 kDefaultBabyScale = 160;   // m = ceil(sqrt(jcount)) x 160/256
+constexpr u32 kDefaultFill = 160;        // fingerprint words: 0.625 keys per word on average
 
 // Item constants, precomputed on the host once per item (all integer, exact).
 struct DevItem {

@@ -29,7 +29,7 @@ constexpr u64 kMaxSplit = 1ull << 28;       // largest split modulus (at most 9 
 // Every prime l of Q with l | p - 1 splits a prime's exponents into l classes
 // and keeps one, so a larger Q leaves fewer BSGS steps (about 1/(l-1) of the
 // primes gain a factor l); the prep pays a longer walk for them.
-constexpr u64 kSplitBases[] = {720720ull, 5040ull};   // 2^4 3^2 5 7 11 13, 2^4 3^2 5 7
+constexpr u64 kSplitBases[] = {232792560ull, 720720ull, 5040ull};   // 2^4 3^2 5 7 11 13 17 19; to 13; to 7
 inline u64 split_modulus(u32 class_modulus, u64 cm) {
     if (class_modulus == 0) {
         for (u64 base : kSplitBases) {

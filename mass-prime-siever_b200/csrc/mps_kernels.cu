@@ -1055,11 +1055,12 @@ __device__ u64 solve_fp64(const Entry& e, u32* tab, u32 tbits, u64* steps_out) {
 // the word's overflow bit, set when a key homed at this word found it full
 // and moved on (linear probing over words).  The home word is the top tw bits
 // of the key's multiplicative hash h, the fingerprint the next 14 bits.  For
-// m baby steps tw = ceil(log2 m), so a word holds 0.5..1 keys on average and
-// fewer than 0.4% of the words overflow.  A probe reads one word and tests the
-// four halves at once (x = word ^ pattern has a zero 16-bit half exactly when
-// a half matches: (x - 0x0001..) & ~x & 0x8000.. is then nonzero); a home
-// with its overflow bit set also counts as a candidate.  Candidates leave the
+// m baby steps tw = ceil(log2(m * 256 / fill)), so a word holds at most
+// fill/256 keys on average (fill 160: 0.6, and about 0.1% of the words
+// overflow).  A probe reads one word and tests the four halves at once
+// (fq_probe); a home with its overflow bit set also counts as a candidate.
+// The next giant value is multiplied before the probe of the current one, so
+// the multiply's latency overlaps the shared-memory load.  Candidates leave the
 // hot loop: the lane walks the overflow chain, and a fingerprint found is
 // resolved exactly by recomputation (ffind_baby).  Compared with one 32-bit
 // key per slot this stores 2.5x as many baby steps in the same shared memory
@@ -1078,14 +1079,6 @@ constexpr u32 kQOvf = 0x4000u;
 
 __device__ __forceinline__ u32 fq_pattern(u32 h, u32 tw) {
     return ((h >> (18 - tw)) & 0x3FFFu) | 0x8000u;
-}
-
-// Nonzero when a used half of (lo, hi) equals pat, or the word overflowed.
-__device__ __forceinline__ u32 fq_candidate(u32 lo, u32 hi, u32 pat) {
-    const u32 rep = pat * 0x10001u;
-    const u32 x0 = (lo & ~kQOvf) ^ rep, x1 = hi ^ rep;
-    const u32 z = ((x0 - 0x10001u) & ~x0) | ((x1 - 0x10001u) & ~x1);
-    return (z & 0x80008000u) | (lo & kQOvf);
 }
 
 __device__ __forceinline__ bool fq_word_has(u64 w, u32 pat) {
@@ -1126,7 +1119,44 @@ __device__ __forceinline__ bool fq_contains(const unsigned long long* tab, u32 m
     return false;
 }
 
-template <int CH>
+// Warp-cooperative insert (table kind 3): the lanes with want store their
+// (home, pat) into the next free halves of their home words, ranked among the
+// lanes of the warp with the same home (one match, one read, one 16-bit
+// store); a lane whose home word is full takes the atomic walk of fq_insert.
+// The warp owns its table, so plain stores cannot race with other warps.
+__device__ __forceinline__ void fq_insert_warp(unsigned long long* tab, u32 mask, bool want, u32 home, u32 pat) {
+    const u32 lane = threadIdx.x & 31;
+    const u32 peers = __match_any_sync(FULL, want ? home : 0xFFFFFFFFu);
+    bool done = !want;
+    if (want) {
+        const uint2 w = reinterpret_cast<const uint2*>(tab)[home];
+        const u32 used = __popc((w.x & 0x80008000u) | ((w.y & 0x80008000u) >> 1));   // halves fill in order
+        const u32 slot = used + __popc(peers & ((1u << lane) - 1));
+        if (slot < 4) {
+            reinterpret_cast<unsigned short*>(tab)[home * 4 + slot] = (unsigned short)pat;   // bit 14 stays 0
+            done = true;
+        }
+    }
+    __syncwarp();
+    if (!done) fq_insert(tab, mask, home, pat);
+    __syncwarp();
+}
+
+// The probe of a giant value: nonzero when a used half of the home word
+// equals the fingerprint, or the word overflowed.  With x = word ^ pattern
+// (both halves of the pattern), a 16-bit half of x is zero exactly when that
+// half matches, and (x - 0x00010001) & ~x & 0x80008000 is then nonzero.  The
+// caller ORs the probes of its chains and votes once per iteration.
+__device__ __forceinline__ u32 fq_probe(const uint2* t2, u32 h, u32 shift, u32 tw) {
+    const uint2 w = t2[h >> shift];
+    const u32 rep = fq_pattern(h, tw) * 0x10001u;
+    const u32 x0 = (w.x & ~kQOvf) ^ rep, x1 = w.y ^ rep;
+    return (((x0 - 0x10001u) & ~x0) & 0x80008000u) | (((x1 - 0x10001u) & ~x1) & 0x80008000u) | (w.x & kQOvf);
+}
+
+// WI: baby steps inserted by fq_insert_warp (table kind 3) instead of one
+// compare-and-swap each (table kind 0); the table and the probes are the same.
+template <int CH, bool WI>
 __device__ u64 solve_fp64q(const Entry& e, unsigned long long* tab, u32 tbits, u32 fill, u64* steps_out) {
     const u32 lane = threadIdx.x & 31;
     Fp64 f;
@@ -1186,8 +1216,10 @@ __device__ u64 solve_fp64q(const Entry& e, unsigned long long* tab, u32 tbits, u
 #pragma unroll
         for (int c = 0; c < CH; ++c) {
             const u32 i = base + 32 * c + lane;
-            if (i < lim) {
-                const u32 h = fhash(cv[c]);
+            const u32 h = fhash(cv[c]);
+            if (WI) {
+                fq_insert_warp(tab, mask, i < lim, h >> shift, fq_pattern(h, tw));
+            } else if (i < lim) {
                 fq_insert(tab, mask, h >> shift, fq_pattern(h, tw));
             }
         }
@@ -1211,22 +1243,22 @@ __device__ u64 solve_fp64q(const Entry& e, unsigned long long* tab, u32 tbits, u
         giant_done = G;
         const uint2* t2 = reinterpret_cast<const uint2*>(tab);
         for (u32 base = 0; base < G; base += 32 * CH) {
-            double cv[CH];
+            double cv[CH], nx[CH];
             u32 hs[CH];
-            u32 cand = 0;
+            u32 z = 0;
 #pragma unroll
             for (int c = 0; c < CH; ++c) {
                 cv[c] = f.canon(gx[c]);
                 hs[c] = fhash(cv[c]);
-                const uint2 w = t2[hs[c] >> shift];
-                cand |= fq_candidate(w.x, w.y, fq_pattern(hs[c], tw)) ? (1u << c) : 0u;
+                nx[c] = f.mul(gx[c], Gstep);              // the next value, independent of the probe
+                z |= fq_probe(t2, hs[c], shift, tw);
             }
-            if (__any_sync(FULL, cand)) {
+            if (__any_sync(FULL, z)) {
                 // the rare path: walk overflowed homes, then resolve exact matches in increasing g
                 u32 real = 0;
 #pragma unroll
                 for (int c = 0; c < CH; ++c)
-                    if (((cand >> c) & 1u) && base + 32 * c + lane + 1 <= G &&
+                    if (base + 32 * c + lane + 1 <= G && fq_probe(t2, hs[c], shift, tw) &&
                         fq_contains(tab, mask, hs[c] >> shift, fq_pattern(hs[c], tw)))
                         real |= 1u << c;
                 u64 jb = ~0ull;
@@ -1249,7 +1281,7 @@ __device__ u64 solve_fp64q(const Entry& e, unsigned long long* tab, u32 tbits, u
                 }
             }
 #pragma unroll
-            for (int c = 0; c < CH; ++c) gx[c] = f.mul(gx[c], Gstep);
+            for (int c = 0; c < CH; ++c) gx[c] = nx[c];
         }
     }
     __syncwarp();
@@ -1427,170 +1459,12 @@ __device__ u64 solve_fp64h(const Entry& e, unsigned short* tab, u32 tbits, u32 l
     return best < e.jcount ? best : ~0ull;
 }
 
-// ---- the FP64 solve with fingerprint words keyed from the FP64 pipe ----
-//
-// The table of solve_fp64q (four 16-bit fingerprints per 64-bit word, bit 15
-// of a half marks it used, bit 14 of half 0 is the word's overflow bit), with
-// the key taken from the canonical residue's integer: x + 2^52 (one FP64 add)
-// holds x in its low 52 bits, and a multiplicative hash of its two 32-bit
-// words gives the home word (the top bits) and the 14-bit fingerprint (the
-// bits below them), as in solve_fp64q.  Hashing both words matters: residues
-// that are small multiples of powers of two (t * 2^(L i) before the first
-// reduction, b = 2) share their low bits and would pile into one home word.
-// The next giant value is multiplied before the probe of the current one, so
-// the multiply's latency overlaps the shared-memory load and the vote.  A
-// word holds at most 2^-word_shift of the fill on average.
-
-__device__ __forceinline__ u32 xhash_bits(double u) {           // u = x + 2^52, x canonical
-    return (u32)(__double2loint(u) ^ __double2hiint(u)) * kHashMul;
-}
-
-__device__ __forceinline__ u32 xhash(const Fp64& f, double v, double two52) {   // hash of canon(v)
-    double u = __dadd_rn(v, two52);
-    if (v < 0.0) u = __dadd_rn(u, f.p);
-    return xhash_bits(u);
-}
-
-template <int CH>
-__device__ u64 solve_fp64x(const Entry& e, unsigned long long* tab, u32 tbits, u32 load_shift, u32 fill,
-                           u64* steps_out) {
-    const u32 lane = threadIdx.x & 31;
-    const u32 word_shift = load_shift > 2 ? load_shift - 2 : 0;   // slot load 2^-load_shift, four slots a word
-    const double two52 = 4503599627370496.0;
-    Fp64 f;
-    f.init(e.p);
-    const u32 m = e.m;
-    const u32 jc = (u32)e.jcount;                      // jcount <= 10^7
-    // 2^tw words for m keys, within the launch's 2^(tbits-1) words
-    const u32 tw = fq_words_log(m, fill, tbits, word_shift);
-    const u32 mask = (1u << tw) - 1, shift = 32 - tw;
-    const double B = (double)e.B, Bm = (double)e.Bm, tv = (double)e.t, G0 = (double)e.G0;
-
-    double xb = B, xg = Bm;                            // B^(l+1), Bm^(l+1)
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-        const double yb = __shfl_up_sync(FULL, xb, off), yg = __shfl_up_sync(FULL, xg, off);
-        if (lane >= (u32)off) {
-            xb = f.mul(xb, yb);
-            xg = f.mul(xg, yg);
-        }
-    }
-    const double B32 = __shfl_sync(FULL, xb, 31), Bm32 = __shfl_sync(FULL, xg, 31);
-    double bl = __shfl_up_sync(FULL, xb, 1);
-    if (lane == 0) bl = 1.0;
-    double Bstep = B32, Gstep = Bm32;                  // B^(32 CH), Bm^(32 CH)
-#pragma unroll
-    for (int c = 1; c < CH; c <<= 1) {
-        Bstep = f.mul(Bstep, Bstep);
-        Gstep = f.mul(Gstep, Gstep);
-    }
-    const double tbl = f.mul(tv, bl);
-    double bx[CH], gx[CH];
-    bx[0] = tbl;
-    gx[0] = f.mul(G0, xg);
-#pragma unroll
-    for (int c = 1; c < CH; ++c) {
-        bx[c] = f.mul(bx[c - 1], B32);
-        gx[c] = f.mul(gx[c - 1], Bm32);
-    }
-
-    uint4* t4 = reinterpret_cast<uint4*>(tab);
-    for (u32 k = lane; k <= mask / 2; k += 32) t4[k] = make_uint4(0, 0, 0, 0);
-    __syncwarp();
-
-    // baby steps, stopping at a cycle B^d == 1 (d < m)
-    u32 cyc = 0, baby_done = m;
-    for (u32 base = 0; base < m; base += 32 * CH) {
-        double cv[CH], nb[CH];
-        u32 cb = 0;
-#pragma unroll
-        for (int c = 0; c < CH; ++c) {
-            cv[c] = f.canon(bx[c]);
-            nb[c] = f.mul(bx[c], Bstep);
-            const u32 i = base + 32 * c + lane;
-            const u32 bc = __ballot_sync(FULL, i > 0 && i < m && cv[c] == tv);
-            if (bc && !cb) cb = base + 32 * c + __ffs(bc) - 1;
-        }
-        const u32 lim = cb ? cb : m;
-#pragma unroll
-        for (int c = 0; c < CH; ++c) {
-            const u32 i = base + 32 * c + lane;
-            if (i < lim) {
-                const u32 h = xhash_bits(__dadd_rn(cv[c], two52));
-                fq_insert(tab, mask, h >> shift, fq_pattern(h, tw));
-            }
-        }
-        if (cb) {
-            cyc = cb;
-            baby_done = cb;
-            break;
-        }
-#pragma unroll
-        for (int c = 0; c < CH; ++c) bx[c] = nb[c];
-    }
-    __syncwarp();
-
-    u64 best = ~0ull;
-    u32 giant_done = 0;
-    if (cyc) {
-        const int i = ffind_baby(f, tbl, B32, 1, cyc, G0);
-        if (i > 0) best = cyc - (u32)i;
-    } else {
-        const u32 G = (jc - 1 + m - 1) / m;            // g = 1..G covers j in [1, G*m]
-        giant_done = G;
-        const uint2* t2 = reinterpret_cast<const uint2*>(tab);
-        for (u32 base = 0; base < G; base += 32 * CH) {
-            u32 hs[CH];
-            double nx[CH];
-            u32 cand = 0;
-#pragma unroll
-            for (int c = 0; c < CH; ++c) {
-                hs[c] = xhash(f, gx[c], two52);
-                nx[c] = f.mul(gx[c], Gstep);              // the next value, independent of the probe
-                const uint2 w = t2[hs[c] >> shift];
-                cand |= fq_candidate(w.x, w.y, fq_pattern(hs[c], tw)) ? (1u << c) : 0u;
-            }
-            if (__any_sync(FULL, cand)) {
-                u32 real = 0;
-#pragma unroll
-                for (int c = 0; c < CH; ++c)
-                    if (((cand >> c) & 1u) && base + 32 * c + lane + 1 <= G &&
-                        fq_contains(tab, mask, hs[c] >> shift, fq_pattern(hs[c], tw)))
-                        real |= 1u << c;
-                u64 jb = ~0ull;
-#pragma unroll
-                for (int c = 0; c < CH; ++c) {
-                    u32 bb = __ballot_sync(FULL, (real >> c) & 1u);
-                    while (bb && jb == ~0ull) {
-                        const int src = __ffs(bb) - 1;
-                        bb &= bb - 1;
-                        const double v = __shfl_sync(FULL, f.canon(gx[c]), src);
-                        const u64 g = base + 32 * c + (u32)src + 1;
-                        const int i = ffind_baby(f, tbl, B32, 0, m, v);
-                        if (i >= 0) jb = g * m - (u64)i;
-                    }
-                }
-                if (jb != ~0ull) {
-                    best = jb;
-                    giant_done = min(G, base + 32 * CH);
-                    break;
-                }
-            }
-#pragma unroll
-            for (int c = 0; c < CH; ++c) gx[c] = nx[c];
-        }
-    }
-    __syncwarp();
-    if (steps_out) *steps_out = pack_steps(baby_done, giant_done);
-    return best < e.jcount ? best : ~0ull;
-}
-
 template <int CH, int QT>
 __device__ __forceinline__ u64 solve_any(const Entry& e, void* tab, u32 tbits, u32 load_shift, u32 fill, u64* steps) {
     if (CH == 0 || e.p >= kFp64Limit) return solve_entry<FieldM>(e, (unsigned short*)tab, tbits + 1, steps);
-    if (QT == 0) return solve_fp64q<CH ? CH : 1>(e, (unsigned long long*)tab, tbits, fill, steps);
+    if (QT == 0) return solve_fp64q<CH ? CH : 1, false>(e, (unsigned long long*)tab, tbits, fill, steps);
     if (QT == 2) return solve_fp64h<CH ? CH : 1>(e, (unsigned short*)tab, tbits, load_shift, steps);
-    if (QT == 3) return solve_fp64x<CH ? CH : 1>(e, (unsigned long long*)tab, tbits, load_shift, fill, steps);
+    if (QT == 3) return solve_fp64q<CH ? CH : 1, true>(e, (unsigned long long*)tab, tbits, fill, steps);
     return solve_fp64<CH ? CH : 1>(e, (u32*)tab, tbits, steps);
 }
 
@@ -1625,18 +1499,19 @@ __global__ void __launch_bounds__(256, MPS_BSGS_MINB) k_bsgs(BsgsArgs a, Counter
         if (lane == 0 && cur < n_ent) claim = atomicAdd(&ctr->work_next, 1ull);
         u64 stage = cur < n_ent && lane < 9 ? reinterpret_cast<const u64*>(a.ent + cur)[lane] : 0;
         while (cur < n_ent) {
+            // the solve's fields; n_first, L and item are read again for a relation
             Entry e;
             e.p = __shfl_sync(FULL, stage, 0);
             e.t = __shfl_sync(FULL, stage, 1);
             e.G0 = __shfl_sync(FULL, stage, 2);
             e.B = __shfl_sync(FULL, stage, 3);
             e.Bm = __shfl_sync(FULL, stage, 4);
-            e.n_first = __shfl_sync(FULL, stage, 5);
-            e.L = __shfl_sync(FULL, stage, 6);
+            e.n_first = 0;
+            e.L = 0;
             e.jcount = __shfl_sync(FULL, stage, 7);
-            const u64 w8 = __shfl_sync(FULL, stage, 8);
-            e.m = (u32)w8;                                      // little-endian: m, then item
-            e.item = (u32)(w8 >> 32);
+            e.m = (u32)__shfl_sync(FULL, stage, 8);             // little-endian: m, then item
+            e.item = 0;
+            const u64 idx = cur;
             const u64 next = __shfl_sync(FULL, claim, 0);
             stage = next < n_ent && lane < 9 ? reinterpret_cast<const u64*>(a.ent + next)[lane] : 0;
             if (lane == 0 && next < n_ent) claim = atomicAdd(&ctr->work_next, 1ull);
@@ -1648,7 +1523,10 @@ __global__ void __launch_bounds__(256, MPS_BSGS_MINB) k_bsgs(BsgsArgs a, Counter
             u64 steps = 0;
             const u64 j = solve_any<CH, QT>(e, tab, a.tbits, a.load_shift, a.fill, &steps);
             if (lane == 0) {
-                if (j != ~0ull) emit_relation(e.p, e.n_first + j * e.L, 0, e.item, a.rel, a.rel_cap, ctr);
+                if (j != ~0ull) {
+                    const Entry& g = a.ent[idx];
+                    emit_relation(e.p, g.n_first + j * g.L, 0, g.item, a.rel, a.rel_cap, ctr);
+                }
                 my_steps += (steps & 0xFFFFFFFFull) + (steps >> 32);
                 my_baby += steps & 0xFFFFFFFFull;
             }
