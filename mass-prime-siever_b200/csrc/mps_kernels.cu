@@ -401,10 +401,11 @@ __device__ __forceinline__ u32 gcd_Q(const DevItem& it, u64 pm1) {
 // Stage 2: with g = gcd(Q, p - 1) and e = (p - 1) / g, w = b^e and u = t^e
 // are g-th roots of unity and b^n == t forces w^n == u, i.e. n == r (mod d),
 // d = ord(w) -- or there is no solution.  Returns 0 (no solution), 1 (d, r
-// found by a walk of at most `walk` steps) or 2 (longer: deferred).
+// found by a walk of at most `walk` steps) or 2 (longer: deferred, with the
+// residues of w and u in w_out, u_out for stage 2b).
 template <class F>
 __device__ __forceinline__ int power_split(const F& f, u64 p, u64 b_mod, u64 t, const DevItem& it, u32 walk, u32& d,
-                                           u32& r) {
+                                           u32& r, u64& w_out, u64& u_out) {
     typedef typename F::V V;
     const u64 pm1 = p - 1;
     const u32 g = gcd_Q(it, pm1);
@@ -433,19 +434,21 @@ __device__ __forceinline__ int power_split(const F& f, u64 p, u64 b_mod, u64 t, 
             return found ? 1 : 0;
         }
     }
-    return lim == g ? 0 : 2;
+    if (lim == g) return 0;
+    w_out = f.residue(w);
+    u_out = uk;
+    return 2;
 }
 
-// Stage 2b (rare): the same split for long orders, one prime power of g at a
-// time: w_l = w^(g/l^c), u_l = u^(g/l^c) in the l^c-th roots of unity, a walk
-// of at most l^c steps each, combined by the Chinese remainder theorem.
+// Stage 2b: the same split for long orders, one prime power of g at a time,
+// from stage 2's w and u (residues): w_l = w^(g/l^c), u_l = u^(g/l^c) in the
+// l^c-th roots of unity, a walk of at most l^c steps each, combined by the
+// Chinese remainder theorem.
 template <class F>
-__device__ bool power_split_pp(const F& f, u64 p, u64 b_mod, u64 t, const DevItem& it, u32& d, u32& r) {
+__device__ bool power_split_pp(const F& f, u64 p, u64 w_res, u64 u_res, const DevItem& it, u32& d, u32& r) {
     typedef typename F::V V;
-    const u64 pm1 = p - 1;
-    const u32 g = gcd_Q(it, pm1);
-    const u64 e = exact_quotient(pm1, g);
-    const V w = f.pow(f.from_u64(b_mod), e), u = f.pow(f.from_u64(t), e);
+    const u32 g = gcd_Q(it, p - 1);
+    const V w = f.from_u64(w_res), u = f.from_u64(u_res);
     d = 1;
     r = 0;
     for (u32 i = 0; i < it.qf_n; ++i) {
@@ -564,6 +567,7 @@ struct PrepQueues {
     u64 p2[64];
     u32 i2[64], d2[64], r2[64];
     u64 pd[64];
+    u64 wd[64], ud[64];                            // stage 2's w and u of a deferred prime
     u32 id[64];
 };
 
@@ -576,21 +580,19 @@ __device__ __forceinline__ void qpush(bool want, u32& n, u32* slot_out) {
 }
 
 template <class F>
-__device__ __forceinline__ int split_in(const DevItem& it, u64 p, u32& d, u32& r) {
+__device__ __forceinline__ int split_in(const DevItem& it, u64 p, u32& d, u32& r, u64& w, u64& u) {
     F f;
     f.init(p);
     const u64 bm = residue128(it.babs_hi, it.babs_lo, it.b_neg, p);
     const u64 t = p - residue128(it.cabs_hi, it.cabs_lo, it.c_neg, p);
-    return power_split(f, p, bm, t, it, kWalk, d, r);
+    return power_split(f, p, bm, t, it, kWalk, d, r, w, u);
 }
 
 template <class F>
-__device__ __forceinline__ bool split_pp_in(const DevItem& it, u64 p, u32& d, u32& r) {
+__device__ __forceinline__ bool split_pp_in(const DevItem& it, u64 p, u64 w, u64 u, u32& d, u32& r) {
     F f;
     f.init(p);
-    const u64 bm = residue128(it.babs_hi, it.babs_lo, it.b_neg, p);
-    const u64 t = p - residue128(it.cabs_hi, it.cabs_lo, it.c_neg, p);
-    return power_split_pp(f, p, bm, t, it, d, r);
+    return power_split_pp(f, p, w, u, it, d, r);
 }
 
 template <class F>
@@ -635,7 +637,8 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep(PrepArgs a, Counters* ctr
                 p = Q.pd[k];
                 item = Q.id[k];
                 const DevItem& it = a.items[item];
-                ok = p < kFp64Limit ? split_pp_in<FieldF>(it, p, d, r) : split_pp_in<FieldM>(it, p, d, r);
+                const u64 w = Q.wd[k], u = Q.ud[k];
+                ok = p < kFp64Limit ? split_pp_in<FieldF>(it, p, w, u, d, r) : split_pp_in<FieldM>(it, p, w, u, d, r);
             }
             nd -= cnt;
             __syncwarp();
@@ -655,13 +658,13 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep(PrepArgs a, Counters* ctr
             const u32 cnt = min(n1, 32u);
             int res = 0;
             u32 d = 1, r = 0, item = 0;
-            u64 p = 0;
+            u64 p = 0, w = 0, u = 0;
             if (lane < cnt) {
                 const u32 k = n1 - cnt + lane;
                 p = Q.p1[k];
                 item = Q.i1[k];
                 const DevItem& it = a.items[item];
-                res = p < kFp64Limit ? split_in<FieldF>(it, p, d, r) : split_in<FieldM>(it, p, d, r);
+                res = p < kFp64Limit ? split_in<FieldF>(it, p, d, r, w, u) : split_in<FieldM>(it, p, d, r, w, u);
             }
             n1 -= cnt;
             __syncwarp();
@@ -675,6 +678,8 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep(PrepArgs a, Counters* ctr
                 Q.r2[s2] = r;
             } else if (res == 2) {
                 Q.pd[sd] = p;
+                Q.wd[sd] = w;
+                Q.ud[sd] = u;
                 Q.id[sd] = item;
             }
             __syncwarp();
