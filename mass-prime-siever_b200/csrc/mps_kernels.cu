@@ -273,7 +273,9 @@ __global__ void __launch_bounds__(kSieveThreads) k_sieve_wave(const WaveDesc* w,
 
 // Two exact arithmetics behind one interface: FP64 (p < 2^49, the FP64 pipe)
 // and 64-bit Montgomery (p < 2^62, the integer pipe).  V is the value type;
-// key() gives the canonical integer (the table key) of a canonical value.
+// key() gives the canonical integer (the table key) of a canonical value;
+// eq(a, c) compares a product (or one()) with a canonical value c without
+// leaving the field's representation.
 
 struct FieldF {
     typedef double V;
@@ -287,6 +289,7 @@ struct FieldF {
     __device__ __forceinline__ V one() const { return 1.0; }
     __device__ __forceinline__ V dbl(V a) const { return __dadd_rn(a, a); }      // (-p, p) -> (-2p, 2p)
     __device__ __forceinline__ V pow(V b, u64 e) const { return f.pow(b, e); }
+    __device__ __forceinline__ bool eq(V a, V c) const { return a == c || a == c - f.p; }   // a in (-p, p)
 };
 
 struct FieldM {
@@ -305,6 +308,7 @@ struct FieldM {
     __device__ __forceinline__ V one() const { return M.one; }
     __device__ __forceinline__ V dbl(V a) const { return M.dbl(a); }
     __device__ __forceinline__ V pow(V b, u64 e) const { return M.pow(b, e); }
+    __device__ __forceinline__ bool eq(V a, V c) const { return a == c || a == c + M.p; }   // a in [0, 2p)
 };
 
 // --------------------------------------------------------------- the prep --
@@ -419,24 +423,24 @@ __device__ __forceinline__ int power_split(const F& f, u64 p, u64 b_mod, u64 t, 
         bu = f.mul(bu, bu);
         bw = f.mul(bw, bw);
     }
-    const u64 uk = f.residue(u);
-    V x = f.one();
+    const V uc = f.canon(u), one = f.one();
+    V x = one;
     bool found = false;
     const u32 lim = min(g, walk);
     for (u32 k = 0; k < lim; ++k) {                    // discrete log in <w>
-        if (!found && f.residue(x) == uk) {
+        if (!found && f.eq(x, uc)) {
             r = k;
             found = true;
         }
         x = f.mul(x, w);
-        if (f.residue(x) == 1) {
+        if (f.eq(x, one)) {
             d = k + 1;
             return found ? 1 : 0;
         }
     }
     if (lim == g) return 0;
     w_out = f.residue(w);
-    u_out = uk;
+    u_out = f.residue(u);
     return 2;
 }
 
@@ -457,18 +461,17 @@ __device__ bool power_split_pp(const F& f, u64 p, u64 w_res, u64 u_res, const De
         u32 lc = l;
         while (g % (lc * l) == 0) lc *= l;
         const u32 k = g / lc;
-        const V wl = f.pow(w, k), ul = f.pow(u, k);
-        const u64 uk = f.residue(ul);
-        V x = f.one();
+        const V wl = f.pow(w, k), uc = f.canon(f.pow(u, k)), one = f.one();
+        V x = one;
         bool found = false;
         u32 xr = 0, dl = lc;
         for (u32 y = 0; y < lc; ++y) {
-            if (!found && f.residue(x) == uk) {
+            if (!found && f.eq(x, uc)) {
                 xr = y;
                 found = true;
             }
             x = f.mul(x, wl);
-            if (f.residue(x) == 1) {
+            if (f.eq(x, one)) {
                 dl = y + 1;
                 break;
             }
