@@ -372,11 +372,14 @@ def batched_vs_plain(local: int, steps: int, warmup: int, max_width=None, tune: 
         sv.tune_load(tune_file)
         return sv
 
+    stage = {}
+
     def batched(s):
         t0 = time.perf_counter()
         r = s.batch_relations(items)
         wall = time.perf_counter() - t0
         st = s.stats()
+        stage.update({k: st[k] for k in ("sieve_ms", "prep_ms", "bsgs_ms", "order_ms")})
         return r, st["device_ms"] / 1e3, wall, st["kernel_launches"]
 
     def per_item(s):
@@ -431,6 +434,7 @@ def batched_vs_plain(local: int, steps: int, warmup: int, max_width=None, tune: 
         "primes": nprimes, "relations": len(rel_b),
         "batched": {"value": b_rate, "unit": "primes/s", "ms_per_step": dev_b * 1e3 / steps,
                     "e2e": nprimes * steps / wall_b, "gpu_launches": l_b // steps,
+                    "stage_ms_overlapping": stage,
                     "path": "mps_batch_relations: multi-item waves, graph replay, two overlapped slots"},
         "plain_per_item": {"value": nprimes / dev_p, "unit": "primes/s", "ms": dev_p * 1e3, "e2e": nprimes / wall_p,
                            "gpu_launches": l_p,
