@@ -345,8 +345,8 @@ int upload_items(mps_ctx* c, const DevItem* items, size_t n) {
 
 int grid_for(mps_ctx* c, int per_sm) { return c->num_sms * per_sm; }
 
-int bsgs_grid(mps_ctx* c, u32 tbits, u32 warps, int* grid) {
-    const size_t smem = bsgs_smem_bytes(tbits, warps);
+int bsgs_grid(mps_ctx* c, u32 tbits, u32 warps, u32 kind, int* grid) {
+    const size_t smem = bsgs_smem_bytes(tbits, warps, kind);
     if (smem > c->smem_optin) return fail(c, MPS_E_ARG, "baby-step tables exceed shared memory");
     // blocks per SM limited by shared memory (1 KB reserved per block) and 64 warps per SM
     int per_sm = (int)(228 * 1024 / (smem + 1024));
@@ -422,7 +422,7 @@ int run_chunk(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, const LaunchCfg& g_it
     CK(launch_sieve(sa, c->tables(), c->d_surv, nullptr, c->surv_cap, c->d_ctr, s, g.seg_words), "sieve launch");
     CK(cudaEventRecord(c->evk[1], s), "event");
     int bgrid = 0;
-    if (int r = bsgs_grid(c, tbits, warps, &bgrid)) return r;
+    if (int r = bsgs_grid(c, tbits, warps, g.kind, &bgrid)) return r;
     if (c->tun.plain) {
         // the plain path: a host read of each stage's count sizes the next launch
         CK(cudaMemcpyAsync(c->h_ctr, c->d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, s), "count read");
@@ -568,7 +568,7 @@ int slot_enqueue(mps_ctx* c, WaveSlot& w, u32 tbits, const LaunchCfg& g, bool ca
     OrderArgs oa{};
     oa.rel = w.d_rel; oa.rel_cap = w.rel_cap; oa.items = c->d_items; oa.tables = c->tables();
     int bgrid = 0;
-    if (int r = bsgs_grid(c, tbits, warps, &bgrid)) return r;
+    if (int r = bsgs_grid(c, tbits, warps, g.kind, &bgrid)) return r;
     CK(cudaMemcpyAsync(w.d_wave, w.h_wave, sizeof(WaveDesc), cudaMemcpyHostToDevice, s), "wave upload");
     CK(cudaMemsetAsync(w.d_ctr, 0, sizeof(Counters), s), "counter reset");
     // external records: a captured graph records these events on every replay
@@ -606,7 +606,7 @@ int slot_launch(mps_ctx* c, WaveSlot& w, u32 tbits, const LaunchCfg& cfg) {
         if (g.tbits == tbits && g.cfg == cfg) exec = g.exec;
     if (!exec) {
         if (w.graphs.size() >= 8) drop_graphs(w);
-        CK(bsgs_reserve_smem(bsgs_smem_bytes(tbits, cfg.warps)), "bsgs shared memory");
+        CK(bsgs_reserve_smem(bsgs_smem_bytes(tbits, cfg.warps, cfg.kind)), "bsgs shared memory");
         cudaGraph_t g = nullptr;
         CK(cudaStreamBeginCapture(w.stream, cudaStreamCaptureModeThreadLocal), "capture");
         const int r = slot_enqueue(c, w, tbits, cfg, true);
@@ -1324,7 +1324,7 @@ int mps_filter(mps_ctx* c, const uint64_t* primes, size_t n, const mps_item* ite
         table_for(c, g, d.K, &tbits, &mb);
         const u32 warps = g.warps;
         int bgrid = 0;
-        if (int r = bsgs_grid(c, tbits, warps, &bgrid)) return r;
+        if (int r = bsgs_grid(c, tbits, warps, g.kind, &bgrid)) return r;
         cudaStream_t s = c->stream;
         CK(cudaMemsetAsync(c->d_ctr, 0, sizeof(Counters), s), "counter reset");
         CK(cudaMemcpyAsync(c->d_surv, primes + off, cnt * sizeof(u64), cudaMemcpyHostToDevice, s), "prime upload");
@@ -1729,7 +1729,7 @@ int mps_autotune(mps_ctx* c, const mps_item* items, size_t n_items, mps_tune_rep
             table_for(c, g, d.K, &tb, &mb);
             d.max_baby = mb;
             d.baby_scale = g.scale;
-            if (bsgs_smem_bytes(tb, g.warps) > c->smem_optin) continue;
+            if (bsgs_smem_bytes(tb, g.warps, g.kind) > c->smem_optin) continue;
             if (int r = upload_items(c, &d, 1)) return r;
             ++timed;
             double ms = 0, sms = 0;

@@ -1127,27 +1127,39 @@ __device__ __forceinline__ bool fq_contains(const unsigned long long* tab, u32 m
     return false;
 }
 
-// Warp-cooperative insert (table kind 3): the lanes with want store their
-// (home, pat) into the next free halves of their home words, ranked among the
-// lanes of the warp with the same home (one match, one read, one 16-bit
-// store); a lane whose home word is full takes the atomic walk of fq_insert.
-// The warp owns its table, so plain stores cannot race with other warps.
-__device__ __forceinline__ void fq_insert_warp(unsigned long long* tab, u32 mask, bool want, u32 home, u32 pat) {
-    const u32 lane = threadIdx.x & 31;
-    const u32 peers = __match_any_sync(FULL, want ? home : 0xFFFFFFFFu);
-    bool done = !want;
-    if (want) {
-        const uint2 w = reinterpret_cast<const uint2*>(tab)[home];
-        const u32 used = __popc((w.x & 0x80008000u) | ((w.y & 0x80008000u) >> 1));   // halves fill in order
-        const u32 slot = used + __popc(peers & ((1u << lane) - 1));
-        if (slot < 4) {
-            reinterpret_cast<unsigned short*>(tab)[home * 4 + slot] = (unsigned short)pat;   // bit 14 stays 0
-            done = true;
+// Table kind 3: the fingerprint words of kind 0 with a count byte per word
+// (after the launch's words: one byte per eight of table).  The lanes with
+// want claim the next half of their home word by one shared-memory atomic add
+// on its count and write their fingerprints with plain 16-bit stores (every
+// claimed half is distinct); a lane whose word is full (count >= 4) moves on
+// to the next word in the next round, as in kind 0's walk.  The overflow bits
+// of the homes that overflowed are set after every store of the call, so a
+// store to half 0 never clears one.  A count never passes 3 + 32 (it is read
+// before it is raised), so a byte does not wrap.
+__device__ __forceinline__ void fq_insert_count(unsigned long long* tab, unsigned char* cnt, u32 mask, bool want,
+                                                u32 home, u32 pat) {
+    volatile unsigned char* vc = cnt;
+    unsigned short* t16 = reinterpret_cast<unsigned short*>(tab);
+    bool pending = want, ovf = false;
+    u32 s = home;
+    while (__any_sync(FULL, pending)) {
+        if (pending) {
+            u32 k = 4;
+            if (vc[s] < 4u) {
+                const u32 sh = 8u * (s & 3u);
+                k = (atomicAdd(reinterpret_cast<u32*>(cnt) + (s >> 2), 1u << sh) >> sh) & 0xFFu;
+            }
+            if (k < 4u) {
+                t16[4 * s + k] = (unsigned short)pat;
+                pending = false;
+            } else {
+                ovf |= s == home;
+                s = (s + 1) & mask;
+            }
         }
     }
     __syncwarp();
-    if (!done) fq_insert(tab, mask, home, pat);
-    __syncwarp();
+    if (ovf) atomicOr(reinterpret_cast<u32*>(tab) + 2 * home, kQOvf);
 }
 
 // The probe of a giant value: nonzero when a used half of the home word
@@ -1162,8 +1174,9 @@ __device__ __forceinline__ u32 fq_probe(const uint2* t2, u32 h, u32 shift, u32 t
     return (((x0 - 0x10001u) & ~x0) & 0x80008000u) | (((x1 - 0x10001u) & ~x1) & 0x80008000u) | (w.x & kQOvf);
 }
 
-// WI: baby steps inserted by fq_insert_warp (table kind 3) instead of one
-// compare-and-swap each (table kind 0); the table and the probes are the same.
+// WI: baby steps inserted by fq_insert_count (table kind 3, count bytes
+// after the words) instead of one compare-and-swap each (table kind 0); the
+// words and the probes are the same.
 template <int CH, bool WI>
 __device__ u64 solve_fp64q(const Entry& e, unsigned long long* tab, u32 tbits, u32 fill, u64* steps_out) {
     const u32 lane = threadIdx.x & 31;
@@ -1204,21 +1217,32 @@ __device__ u64 solve_fp64q(const Entry& e, unsigned long long* tab, u32 tbits, u
         gx[c] = f.mul(gx[c - 1], Bm32);
     }
 
+    unsigned char* cnt = reinterpret_cast<unsigned char*>(tab) + (4u << tbits);   // kind 3 only
     uint4* t4 = reinterpret_cast<uint4*>(tab);
     for (u32 k = lane; k <= mask / 2; k += 32) t4[k] = make_uint4(0, 0, 0, 0);
+    if (WI)
+        for (u32 k = lane; k <= mask / 16; k += 32) reinterpret_cast<uint4*>(cnt)[k] = make_uint4(0, 0, 0, 0);
     __syncwarp();
 
-    // baby steps, stopping at a cycle B^d == 1 (d < m)
+    // baby steps, stopping at a cycle B^d == 1 (d < m): t B^i == t for an
+    // i in [1, m) is looked for with one vote per iteration, and located
+    // exactly only when one is found
     u32 cyc = 0, baby_done = m;
     for (u32 base = 0; base < m; base += 32 * CH) {
         double cv[CH];
-        u32 cb = 0;
+        bool hit = false;
 #pragma unroll
         for (int c = 0; c < CH; ++c) {
             cv[c] = f.canon(bx[c]);
-            const u32 i = base + 32 * c + lane;
-            const u32 bc = __ballot_sync(FULL, i > 0 && i < m && cv[c] == tv);
-            if (bc && !cb) cb = base + 32 * c + __ffs(bc) - 1;
+            hit |= base + 32 * c + lane - 1u < m - 1u && cv[c] == tv;
+        }
+        u32 cb = 0;
+        if (__any_sync(FULL, hit)) {
+#pragma unroll
+            for (int c = 0; c < CH; ++c) {
+                const u32 bc = __ballot_sync(FULL, base + 32 * c + lane - 1u < m - 1u && cv[c] == tv);
+                if (bc && !cb) cb = base + 32 * c + __ffs(bc) - 1;
+            }
         }
         const u32 lim = cb ? cb : m;
 #pragma unroll
@@ -1226,7 +1250,7 @@ __device__ u64 solve_fp64q(const Entry& e, unsigned long long* tab, u32 tbits, u
             const u32 i = base + 32 * c + lane;
             const u32 h = fhash(cv[c]);
             if (WI) {
-                fq_insert_warp(tab, mask, i < lim, h >> shift, fq_pattern(h, tw));
+                fq_insert_count(tab, cnt, mask, i < lim, h >> shift, fq_pattern(h, tw));
             } else if (i < lim) {
                 fq_insert(tab, mask, h >> shift, fq_pattern(h, tw));
             }
@@ -1492,7 +1516,8 @@ template <int CH, int QT>
 __global__ void __launch_bounds__(256, MPS_BSGS_MINB) k_bsgs(BsgsArgs a, Counters* ctr) {
     extern __shared__ __align__(16) u32 smem32[];
     const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    u32* tab = smem32 + (size_t)warp * (1u << a.tbits);
+    // per warp 4 << tbits bytes of table (kind 3: and one count byte per eight)
+    u32* tab = smem32 + (size_t)warp * ((1u << a.tbits) + (QT == 3 ? (1u << a.tbits) / 8 : 0u));
     const u64 n_ent = min((u64)*(volatile unsigned long long*)&ctr->entries, a.ent_cap);
     u64 my_steps = 0, my_baby = 0;
     if (a.persistent) {
@@ -2119,7 +2144,10 @@ __global__ void k_order_direct(const u64* bp, u64* q_out, u64 count, SieveTables
 
 // -------------------------------------------------------------- launchers --
 
-size_t bsgs_smem_bytes(u32 tbits, u32 warps_per_block) { return (size_t)warps_per_block * (4u << tbits); }
+size_t bsgs_smem_bytes(u32 tbits, u32 warps_per_block, u32 table_kind) {
+    const size_t per_warp = (size_t)(4u << tbits);
+    return (size_t)warps_per_block * (table_kind == 3 ? per_warp + per_warp / 8 : per_warp);
+}
 
 bool valid_seg_words(u32 seg_words) { return seg_words == 1024 || seg_words == 2048 || seg_words == 4096; }
 
@@ -2175,7 +2203,8 @@ cudaError_t bsgs_reserve_smem(size_t smem) {
 }
 
 cudaError_t launch_bsgs(const BsgsArgs& a, Counters* ctr, int grid, cudaStream_t s) {
-    const size_t smem = bsgs_smem_bytes(a.tbits, a.warps_per_block);
+    const size_t smem = bsgs_smem_bytes(a.tbits, a.warps_per_block,
+                                        a.max_p >= kFp64Limit || (a.table_kind == 2 && a.lanes != 32) ? 0 : a.table_kind);
     cudaError_t err = bsgs_reserve_smem(smem);
     if (err != cudaSuccess) return err;
     auto go = [&](auto kern) {
@@ -2257,7 +2286,7 @@ cudaError_t launch_is_prime(const u64* n, u32* out, u64 count, cudaStream_t s) {
 
 cudaError_t launch_bsgs_direct(const u64* cases, u64* j_out, u64 count, u32 tbits, u32 table_kind, cudaStream_t s) {
     if (count == 0) return cudaSuccess;
-    const size_t smem = (size_t)4 << tbits;
+    const size_t smem = bsgs_smem_bytes(tbits, 1, table_kind);
     cudaError_t err = cudaFuncSetAttribute(k_bsgs_direct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
     k_bsgs_direct<<<(unsigned)count, 32, smem, s>>>(cases, j_out, count, tbits, table_kind);

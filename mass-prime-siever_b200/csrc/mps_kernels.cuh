@@ -134,6 +134,8 @@ cudaError_t launch_bsgs_direct(const u64* cases /* p,B,G0,t,jcount */, u64* j_ou
 cudaError_t launch_order_direct(const u64* bp /* b,p pairs */, u64* q_out, u64 count, SieveTables t,
                                 cudaStream_t s);
 
-size_t bsgs_smem_bytes(u32 tbits, u32 warps_per_block);
+// Dynamic shared memory of a BSGS launch: 4 << tbits bytes of table per warp,
+// and for table kind 3 one count byte per eight bytes of table.
+size_t bsgs_smem_bytes(u32 tbits, u32 warps_per_block, u32 table_kind);
 
 }  // namespace mps

@@ -201,7 +201,7 @@ int run_pass(unsigned char* base, u64 lo, u64 hi, const DevItem& d, u32 tbits, i
     oa.items = ditem;
     oa.tables = tables;
 
-    const size_t smem = bsgs_smem_bytes(tbits, 4);
+    const size_t smem = bsgs_smem_bytes(tbits, 4, 0);
     const int bgrid = num_sms * std::max(1, std::min((int)(228 * 1024 / (smem + 1024)), 16));
     if (cudaMemsetAsync(ctr, 0, sizeof(Counters), s) != cudaSuccess) return MPS_E_CUDA;
     if (cudaMemcpyAsync(ditem, &d, sizeof(DevItem), cudaMemcpyHostToDevice, s) != cudaSuccess) return MPS_E_CUDA;
