@@ -395,6 +395,7 @@ int run_chunk(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, const LaunchCfg& g_it
     pa.rel_cap = c->rel_cap;
     pa.full_mr = c->tun.full_mr;
     pa.m_cap = launch_m_cap(c, g, tbits);
+    pa.m_round = g.lanes * g.chains;
 
     BsgsArgs ba{};
     ba.ent = c->d_ent;
@@ -560,6 +561,7 @@ int slot_enqueue(mps_ctx* c, WaveSlot& w, u32 tbits, const LaunchCfg& g, bool ca
     pa.items = c->d_items; pa.ent = w.d_ent; pa.ent_cap = w.ent_cap; pa.rel = w.d_rel; pa.rel_cap = w.rel_cap;
     pa.full_mr = c->tun.full_mr;
     pa.m_cap = launch_m_cap(c, g, tbits);
+    pa.m_round = g.lanes * g.chains;
     BsgsArgs ba{};
     ba.ent = w.d_ent; ba.ent_cap = w.ent_cap; ba.rel = w.d_rel; ba.rel_cap = w.rel_cap; ba.tbits = tbits;
     ba.warps_per_block = warps; ba.persistent = 1; ba.chains = g.chains;
@@ -1335,6 +1337,7 @@ int mps_filter(mps_ctx* c, const uint64_t* primes, size_t n, const mps_item* ite
         pa.surv = c->d_surv; pa.surv_cap = c->surv_cap; pa.item0 = 0; pa.items = c->d_items;
         pa.ent = c->d_ent; pa.ent_cap = c->ent_cap; pa.rel = c->d_rel; pa.rel_cap = c->rel_cap; pa.full_mr = c->tun.full_mr;
         pa.m_cap = launch_m_cap(c, g, tbits);
+        pa.m_round = g.lanes * g.chains;
         BsgsArgs ba{};
         ba.ent = c->d_ent; ba.ent_cap = c->ent_cap; ba.rel = c->d_rel; ba.rel_cap = c->rel_cap;
         ba.tbits = tbits; ba.warps_per_block = warps; ba.persistent = 1; ba.chains = g.chains; ba.table_kind = g.kind;

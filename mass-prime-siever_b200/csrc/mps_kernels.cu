@@ -516,6 +516,9 @@ __device__ void bsgs_setup(const F& f, u64 p, u64 b_mod, u64 t, const DevItem& i
     const V Bv = f.pow(bv, L);
     u32 m = (u32)isqrt_ceil_dev(jcount);
     if (it.baby_scale != 256) m = max(1u, (u32)(((u64)m * it.baby_scale + 255) >> 8));
+    // a whole number of baby iterations (lanes x chains per prime): the last
+    // iteration's lanes then all insert, and the extra baby steps save giant steps
+    if (a.m_round > 1) m = (m + a.m_round - 1) / a.m_round * a.m_round;
     if (m > it.max_baby) m = it.max_baby;
     if (m > a.m_cap) m = a.m_cap;                      // never more than the launch's tables hold
     const u64 Bm = f.residue(f.pow(Bv, m));
@@ -1128,38 +1131,45 @@ __device__ __forceinline__ bool fq_contains(const unsigned long long* tab, u32 m
 }
 
 // Table kind 3: the fingerprint words of kind 0 with a count byte per word
-// (after the launch's words: one byte per eight of table).  The lanes with
-// want claim the next half of their home word by one shared-memory atomic add
-// on its count and write their fingerprints with plain 16-bit stores (every
-// claimed half is distinct); a lane whose word is full (count >= 4) moves on
-// to the next word in the next round, as in kind 0's walk.  The overflow bits
-// of the homes that overflowed are set after every store of the call, so a
-// store to half 0 never clears one.  A count never passes 3 + 32 (it is read
-// before it is raised), so a byte does not wrap.
-__device__ __forceinline__ void fq_insert_count(unsigned long long* tab, unsigned char* cnt, u32 mask, bool want,
-                                                u32 home, u32 pat) {
+// (after the launch's words: one byte per eight of table).  Every chain's key
+// with want claims the next half of its home word by one shared-memory atomic
+// add on the word's count and writes its fingerprint with a plain 16-bit
+// store (every claimed half is distinct); a key whose word is full (count
+// >= 4) moves on to the next word in the next round, as in kind 0's walk.
+// The overflow bits of the homes that overflowed are set after every store of
+// the call, so a store to half 0 never clears one.  A count is read before it
+// is raised, so it never passes 3 + 32 * CH and a byte does not wrap.
+template <int CH>
+__device__ __forceinline__ void fq_insert_count(unsigned long long* tab, unsigned char* cnt, u32 mask, u32 want,
+                                                const u32 (&home)[CH], const u32 (&pat)[CH]) {
     volatile unsigned char* vc = cnt;
     unsigned short* t16 = reinterpret_cast<unsigned short*>(tab);
-    bool pending = want, ovf = false;
-    u32 s = home;
-    while (__any_sync(FULL, pending)) {
-        if (pending) {
+    u32 pend = want, ovf = 0;                          // bit c: chain c
+    u32 s[CH];
+#pragma unroll
+    for (int c = 0; c < CH; ++c) s[c] = home[c];
+    while (__any_sync(FULL, pend)) {
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            if (!((pend >> c) & 1u)) continue;
             u32 k = 4;
-            if (vc[s] < 4u) {
-                const u32 sh = 8u * (s & 3u);
-                k = (atomicAdd(reinterpret_cast<u32*>(cnt) + (s >> 2), 1u << sh) >> sh) & 0xFFu;
+            if (vc[s[c]] < 4u) {
+                const u32 sh = 8u * (s[c] & 3u);
+                k = (atomicAdd(reinterpret_cast<u32*>(cnt) + (s[c] >> 2), 1u << sh) >> sh) & 0xFFu;
             }
             if (k < 4u) {
-                t16[4 * s + k] = (unsigned short)pat;
-                pending = false;
+                t16[4 * s[c] + k] = (unsigned short)pat[c];
+                pend &= ~(1u << c);
             } else {
-                ovf |= s == home;
-                s = (s + 1) & mask;
+                if (s[c] == home[c]) ovf |= 1u << c;
+                s[c] = (s[c] + 1) & mask;
             }
         }
     }
     __syncwarp();
-    if (ovf) atomicOr(reinterpret_cast<u32*>(tab) + 2 * home, kQOvf);
+#pragma unroll
+    for (int c = 0; c < CH; ++c)
+        if ((ovf >> c) & 1u) atomicOr(reinterpret_cast<u32*>(tab) + 2 * home[c], kQOvf);
 }
 
 // The probe of a giant value: nonzero when a used half of the home word
@@ -1229,11 +1239,12 @@ __device__ u64 solve_fp64q(const Entry& e, unsigned long long* tab, u32 tbits, u
     // exactly only when one is found
     u32 cyc = 0, baby_done = m;
     for (u32 base = 0; base < m; base += 32 * CH) {
-        double cv[CH];
+        double cv[CH], nb[CH];
         bool hit = false;
 #pragma unroll
         for (int c = 0; c < CH; ++c) {
             cv[c] = f.canon(bx[c]);
+            nb[c] = f.mul(bx[c], Bstep);                   // the next value, independent of the insert
             hit |= base + 32 * c + lane - 1u < m - 1u && cv[c] == tv;
         }
         u32 cb = 0;
@@ -1245,14 +1256,21 @@ __device__ u64 solve_fp64q(const Entry& e, unsigned long long* tab, u32 tbits, u
             }
         }
         const u32 lim = cb ? cb : m;
+        if (WI) {
+            u32 home[CH], pat[CH], want = 0;
 #pragma unroll
-        for (int c = 0; c < CH; ++c) {
-            const u32 i = base + 32 * c + lane;
-            const u32 h = fhash(cv[c]);
-            if (WI) {
-                fq_insert_count(tab, cnt, mask, i < lim, h >> shift, fq_pattern(h, tw));
-            } else if (i < lim) {
-                fq_insert(tab, mask, h >> shift, fq_pattern(h, tw));
+            for (int c = 0; c < CH; ++c) {
+                const u32 h = fhash(cv[c]);
+                home[c] = h >> shift;
+                pat[c] = fq_pattern(h, tw);
+                if (base + 32 * c + lane < lim) want |= 1u << c;
+            }
+            fq_insert_count<CH>(tab, cnt, mask, want, home, pat);
+        } else {
+#pragma unroll
+            for (int c = 0; c < CH; ++c) {
+                const u32 h = fhash(cv[c]);
+                if (base + 32 * c + lane < lim) fq_insert(tab, mask, h >> shift, fq_pattern(h, tw));
             }
         }
         if (cb) {
@@ -1261,7 +1279,7 @@ __device__ u64 solve_fp64q(const Entry& e, unsigned long long* tab, u32 tbits, u
             break;
         }
 #pragma unroll
-        for (int c = 0; c < CH; ++c) bx[c] = f.mul(bx[c], Bstep);
+        for (int c = 0; c < CH; ++c) bx[c] = nb[c];
     }
     __syncwarp();
 

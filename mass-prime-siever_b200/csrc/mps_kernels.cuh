@@ -84,6 +84,7 @@ struct PrepArgs {
     u64 rel_cap;
     u32 full_mr;               // 1: 12-base Miller-Rabin on every survivor that passes the filters
     u32 m_cap;                 // baby steps per prime at most (what the launch's BSGS tables hold)
+    u32 m_round;               // baby steps rounded up to a multiple of this (the BSGS iteration width)
 };
 cudaError_t launch_prep(const PrepArgs& a, Counters* ctr, int grid, cudaStream_t s);
 
