@@ -58,7 +58,8 @@ typedef struct mps_relation {
     uint64_t p, M, q;
 } mps_relation;
 
-/* Tuning; zero fields take the defaults.  Every setting gives the same relations. */
+/* Tuning; mps_tuning_default fills the defaults (zero fields take them too, except table_kind,
+ * whose zero is a kind of its own).  Every setting gives the same relations. */
 typedef struct mps_tuning {
     uint32_t struct_size;       /* sizeof(mps_tuning)                                          */
     uint32_t table_bits;        /* baby-step table of 2^bits slots per prime (0: per item)     */
@@ -74,10 +75,10 @@ typedef struct mps_tuning {
     uint32_t chains;            /* BSGS chains per lane, 1, 2 or 4 (0: 2)                      */
     uint32_t graphs_off;        /* 1: launch waves directly instead of replaying CUDA graphs   */
     uint32_t table_kind;        /* BSGS table: 0 = four 16-bit fingerprints per 64-bit word,
-                                   1 = one 32-bit key per slot, 2 = one 16-bit fingerprint
-                                   per slot, read with one 16-bit load per probe, 3 = the
-                                   words of 0 filled by warp-cooperative stores (a
-                                   compare-and-swap only when a word is full)               */
+                                   inserted by compare-and-swap, 1 = one 32-bit key per slot,
+                                   2 = one 16-bit fingerprint per slot, read with one 16-bit
+                                   load per probe, 3 = the words of 0 with a count byte per
+                                   word, a half claimed by one atomic add (the default)     */
     uint32_t load_shift;        /* table kind 2: a prime's table has at least 2^load_shift
                                    slots per baby step (0: 2)                                   */
     uint32_t lanes;             /* table kind 2: lanes per prime, 32, 16 or 8 (0: 32); groups of
@@ -257,8 +258,10 @@ int mps_measure_smem_peak(mps_ctx* ctx, double* atomic_or_per_s);
  * For callers that cannot allocate device memory where they sieve: their
  * device memory belongs to another framework's pool allocator, or cudaMalloc
  * / cudaFree (which synchronise the device) are not allowed in their loop.
- * Same relations as mps_chunk_relations with the default tuning, on the
- * calling thread's current device and its per-thread default stream
+ * Same relations as mps_chunk_relations with the default tuning (its BSGS
+ * runs table kind 0, which needs no count bytes, with the default fill and
+ * baby-step scale), on the calling thread's current device and its
+ * per-thread default stream
  * (cudaStreamPerThread), with no context.  All scratch is one static device
  * array of 8 MiB that every GPU loading this library holds until exit; its
  * address is looked up on the first call on each device (make that first

@@ -1176,6 +1176,7 @@ int mps_tuning_default(mps_tuning* t) {
     t->struct_size = sizeof(mps_tuning);
     t->chunk_odds = 1ull << 26;
     t->bsgs_warps = 4;
+    t->table_kind = 3;          // fingerprint words with count-byte claims (fastest measured on the B200)
     return MPS_OK;
 }
 

@@ -45,7 +45,7 @@ def test_abi_version_and_defaults(mps_lib):
     assert lib.mps_abi_version() == 1
     t = mps_lib.default_tuning()
     assert t.struct_size == ctypes.sizeof(mps_lib.Tuning)
-    assert t.chunk_odds == 1 << 26 and t.bsgs_warps == 4
+    assert t.chunk_odds == 1 << 26 and t.bsgs_warps == 4 and t.table_kind == 3
 
 
 def test_open_without_device_is_an_error_not_a_crash(mps_lib):
