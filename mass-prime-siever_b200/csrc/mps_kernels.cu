@@ -1138,27 +1138,32 @@ __device__ __forceinline__ bool fq_contains(const unsigned long long* tab, u32 m
 // >= 4) moves on to the next word in the next round, as in kind 0's walk.
 // The overflow bits of the homes that overflowed are set after every store of
 // the call, so a store to half 0 never clears one.  A count is read before it
-// is raised, so it never passes 3 + 32 * CH and a byte does not wrap.
+// is raised (a stale read only errs low), so it never passes 3 + 32 * CH and a
+// byte does not wrap.  Each round reads the counts of every chain, then
+// issues every claim, then stores, so the chains' latencies overlap.
 template <int CH>
 __device__ __forceinline__ void fq_insert_count(unsigned long long* tab, unsigned char* cnt, u32 mask, u32 want,
                                                 const u32 (&home)[CH], const u32 (&pat)[CH]) {
-    volatile unsigned char* vc = cnt;
     unsigned short* t16 = reinterpret_cast<unsigned short*>(tab);
     u32 pend = want, ovf = 0;                          // bit c: chain c
     u32 s[CH];
 #pragma unroll
     for (int c = 0; c < CH; ++c) s[c] = home[c];
     while (__any_sync(FULL, pend)) {
+        u32 k[CH];
+#pragma unroll
+        for (int c = 0; c < CH; ++c) k[c] = (pend >> c) & 1u ? cnt[s[c]] : 4u;
+#pragma unroll
+        for (int c = 0; c < CH; ++c)
+            if (k[c] < 4u) {
+                const u32 sh = 8u * (s[c] & 3u);
+                k[c] = (atomicAdd(reinterpret_cast<u32*>(cnt) + (s[c] >> 2), 1u << sh) >> sh) & 0xFFu;
+            }
 #pragma unroll
         for (int c = 0; c < CH; ++c) {
             if (!((pend >> c) & 1u)) continue;
-            u32 k = 4;
-            if (vc[s[c]] < 4u) {
-                const u32 sh = 8u * (s[c] & 3u);
-                k = (atomicAdd(reinterpret_cast<u32*>(cnt) + (s[c] >> 2), 1u << sh) >> sh) & 0xFFu;
-            }
-            if (k < 4u) {
-                t16[4 * s[c] + k] = (unsigned short)pat[c];
+            if (k[c] < 4u) {
+                t16[4 * s[c] + k[c]] = (unsigned short)pat[c];
                 pend &= ~(1u << c);
             } else {
                 if (s[c] == home[c]) ovf |= 1u << c;
