@@ -1710,14 +1710,22 @@ __global__ void __launch_bounds__(256, MPS_BSGS_MINB) k_bsgs_groups(BsgsArgs a, 
         bool bdone = m == 0;
         const u32 m_max = __reduce_max_sync(FULL, m);
         for (u32 base = 0; base < m_max; base += L * CH) {
-            double cv[CH];
-            u32 cb = 0;
+            double cv[CH], nb[CH];
+            bool hit = false;
 #pragma unroll
             for (int c = 0; c < CH; ++c) {
                 cv[c] = f.canon(bx[c]);
-                const u32 i = base + L * c + gl;
-                const u32 gb = (__ballot_sync(FULL, !bdone && i > 0 && i < m && cv[c] == tv) >> gshift) & gbits;
-                if (gb && !cb) cb = base + L * c + __ffs(gb) - 1;
+                nb[c] = f.mul(bx[c], Bstep);               // the next value, independent of the inserts
+                hit |= !bdone && base + L * c + gl - 1u < m - 1u && cv[c] == tv;
+            }
+            u32 cb = 0;
+            if (__any_sync(FULL, hit)) {                    // a cycle in some group: locate it exactly
+#pragma unroll
+                for (int c = 0; c < CH; ++c) {
+                    const u32 i = base + L * c + gl;
+                    const u32 gb = (__ballot_sync(FULL, !bdone && i > 0 && i < m && cv[c] == tv) >> gshift) & gbits;
+                    if (gb && !cb) cb = base + L * c + __ffs(gb) - 1;
+                }
             }
             const u32 lim = cb ? cb : m;
 #pragma unroll
@@ -1730,7 +1738,7 @@ __global__ void __launch_bounds__(256, MPS_BSGS_MINB) k_bsgs_groups(BsgsArgs a, 
             bdone = bdone || cb != 0 || base + L * CH >= m;
             if (__all_sync(FULL, bdone)) break;
 #pragma unroll
-            for (int c = 0; c < CH; ++c) bx[c] = f.mul(bx[c], Bstep);
+            for (int c = 0; c < CH; ++c) bx[c] = nb[c];
         }
         __syncwarp();
 
@@ -1746,10 +1754,12 @@ __global__ void __launch_bounds__(256, MPS_BSGS_MINB) k_bsgs_groups(BsgsArgs a, 
         const u32 G_max = __reduce_max_sync(FULL, G);
         for (u32 base = 0; base < G_max; base += L * CH) {
             u32 hs[CH];
+            double nx[CH];
             bool flag = false;
 #pragma unroll
             for (int c = 0; c < CH; ++c) {
                 hs[c] = hkey_canon(f.canon(gx[c]));
+                nx[c] = f.mul(gx[c], Gstep);                   // the next value, independent of the probe
                 const u32 slot = tab[hs[c] >> shift];
                 flag |= !gdone && ((((slot ^ hfp(hs[c])) & 0x7FFFu) == 0) | ((slot & 0x8000u) != 0));
             }
@@ -1783,7 +1793,7 @@ __global__ void __launch_bounds__(256, MPS_BSGS_MINB) k_bsgs_groups(BsgsArgs a, 
             gdone = gdone || base + L * CH >= G;
             if (__all_sync(FULL, gdone)) break;
 #pragma unroll
-            for (int c = 0; c < CH; ++c) gx[c] = f.mul(gx[c], Gstep);
+            for (int c = 0; c < CH; ++c) gx[c] = nx[c];
         }
         __syncwarp();
         if (gl == 0 && active) {
