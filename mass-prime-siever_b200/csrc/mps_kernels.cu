@@ -1134,31 +1134,42 @@ __device__ __forceinline__ bool fq_contains(const unsigned long long* tab, u32 m
 // (after the launch's words: one byte per eight of table).  Every chain's key
 // with want claims the next half of its home word by one shared-memory atomic
 // add on the word's count and writes its fingerprint with a plain 16-bit
-// store (every claimed half is distinct); a key whose word is full (count
-// >= 4) moves on to the next word in the next round, as in kind 0's walk.
-// The overflow bits of the homes that overflowed are set after every store of
-// the call, so a store to half 0 never clears one.  A count is read before it
-// is raised (a stale read only errs low), so it never passes 3 + 32 * CH and a
-// byte does not wrap.  Each round reads the counts of every chain, then
-// issues every claim, then stores, so the chains' latencies overlap.
+// store (every claimed half is distinct).  A claim that finds the word full
+// (count >= 4) is taken back at once, so a count rests at 4 at most and never
+// passes 4 + 32 * CH in flight (a byte cannot wrap).  The rare keys whose home
+// was full then walk on, word by word, in rounds of the whole warp, as in
+// kind 0's walk; the overflow bits of their homes are set after every store
+// of the call, so a store to half 0 never clears one.
+__device__ __forceinline__ u32 fq_claim(unsigned char* cnt, u32 s) {
+    const u32 sh = 8u * (s & 3u);
+    u32* c32 = reinterpret_cast<u32*>(cnt) + (s >> 2);
+    const u32 k = (atomicAdd(c32, 1u << sh) >> sh) & 0xFFu;
+    if (k >= 4u) atomicSub(c32, 1u << sh);          // full: take the claim back
+    return k;
+}
+
 template <int CH>
 __device__ __forceinline__ void fq_insert_count(unsigned long long* tab, unsigned char* cnt, u32 mask, u32 want,
                                                 const u32 (&home)[CH], const u32 (&pat)[CH]) {
     unsigned short* t16 = reinterpret_cast<unsigned short*>(tab);
-    u32 pend = want, ovf = 0;                          // bit c: chain c
+    u32 k[CH];
+#pragma unroll
+    for (int c = 0; c < CH; ++c) k[c] = (want >> c) & 1u ? fq_claim(cnt, home[c]) : 0u;
+    u32 pend = 0;                                      // bit c: chain c found its home full
+#pragma unroll
+    for (int c = 0; c < CH; ++c) {
+        if (!((want >> c) & 1u)) continue;
+        if (k[c] < 4u) t16[4 * home[c] + k[c]] = (unsigned short)pat[c];
+        else pend |= 1u << c;
+    }
+    if (!__any_sync(FULL, pend)) return;
+    const u32 ovf = pend;
     u32 s[CH];
 #pragma unroll
-    for (int c = 0; c < CH; ++c) s[c] = home[c];
+    for (int c = 0; c < CH; ++c) s[c] = (home[c] + 1) & mask;
     while (__any_sync(FULL, pend)) {
-        u32 k[CH];
 #pragma unroll
-        for (int c = 0; c < CH; ++c) k[c] = (pend >> c) & 1u ? cnt[s[c]] : 4u;
-#pragma unroll
-        for (int c = 0; c < CH; ++c)
-            if (k[c] < 4u) {
-                const u32 sh = 8u * (s[c] & 3u);
-                k[c] = (atomicAdd(reinterpret_cast<u32*>(cnt) + (s[c] >> 2), 1u << sh) >> sh) & 0xFFu;
-            }
+        for (int c = 0; c < CH; ++c) k[c] = (pend >> c) & 1u ? fq_claim(cnt, s[c]) : 4u;
 #pragma unroll
         for (int c = 0; c < CH; ++c) {
             if (!((pend >> c) & 1u)) continue;
@@ -1166,7 +1177,6 @@ __device__ __forceinline__ void fq_insert_count(unsigned long long* tab, unsigne
                 t16[4 * s[c] + k[c]] = (unsigned short)pat[c];
                 pend &= ~(1u << c);
             } else {
-                if (s[c] == home[c]) ovf |= 1u << c;
                 s[c] = (s[c] + 1) & mask;
             }
         }
