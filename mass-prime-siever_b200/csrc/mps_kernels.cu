@@ -1083,8 +1083,10 @@ constexpr u64 kQValid = 0x8000800080008000ull;
 // words (fill 1..256; 0 counts as 256) and at least 32, at most 2^(tbits-1).
 __device__ __forceinline__ u32 fq_words_log(u32 m, u32 fill, u32 tbits, u32 extra_shift) {
     const u32 f = fill - 1u < 256u ? fill : 256u;
-    const u32 need = (u32)(((u64)max(m, 2u) * 256u + f - 1) / f);
-    return min(tbits - 1, max(5u, 32u - __clz(need - 1) + extra_shift));
+    const u32 keys = max(m, 2u) * 256u;                // m <= 4096: fits 32 bits
+    u32 t = 32u - __clz(max(m, 2u) - 1);               // 2^t >= m; 2^t f >= 256 m needs at most 8 more
+    while ((f << t) < keys) ++t;                       // no division: f << t <= 2^28
+    return min(tbits - 1, max(5u, t + extra_shift));
 }
 constexpr u32 kQOvf = 0x4000u;
 
@@ -1244,6 +1246,7 @@ __device__ u64 solve_fp64q(const Entry& e, unsigned long long* tab, u32 tbits, u
 
     unsigned char* cnt = reinterpret_cast<unsigned char*>(tab) + (4u << tbits);   // kind 3 only
     uint4* t4 = reinterpret_cast<uint4*>(tab);
+#pragma unroll 4
     for (u32 k = lane; k <= mask / 2; k += 32) t4[k] = make_uint4(0, 0, 0, 0);
     if (WI)
         for (u32 k = lane; k <= mask / 16; k += 32) reinterpret_cast<uint4*>(cnt)[k] = make_uint4(0, 0, 0, 0);
