@@ -1829,37 +1829,42 @@ __device__ __forceinline__ u64 rho_step(const Mont& R, u64 y, u64 c) {
     return z >= R.p ? z - R.p : z;
 }
 
-// Pollard-Brent rho on an odd composite n < 2^62 (Montgomery steps); returns
-// a nontrivial factor, or 0 after a bounded number of tries.
-__device__ u64 rho_factor(u64 n) {
+// Pollard-Brent rho with the 32 lanes of a warp walking 32 different maps
+// y -> y^2 + c (c = c0 + lane) in lockstep; the first lane whose batch gcd
+// gives a nontrivial factor wins (a batch that overshoots to n is replayed
+// step by step from its start).  Returns a nontrivial factor of the odd
+// composite n < 2^62, or 0 after four rounds of 32 maps.  Warp-uniform.
+__device__ u64 warp_rho_factor(u64 n) {
+    const u32 lane = threadIdx.x & 31;
     Mont R;
     R.init(n);
-    for (u64 c = 1; c < 64; ++c) {
-        u64 y = R.one, q = R.one, g = 1, x = 0, ys = 0;
-        u64 r = 1;
-        const u64 step_cap = 1ull << 24;
-        while (g == 1 && r <= step_cap) {
-            x = y;
+    for (u64 c0 = 1; c0 < 1 + 32 * 4; c0 += 32) {
+        const u64 c = c0 + lane;
+        u64 y = R.one, q = R.one, x = 0, ys = 0, g = 1;
+        bool stop = false;
+        for (u64 r = 1; r <= (1ull << 24) && !stop; r <<= 1) {
+            if (g == 1) x = y;                         // a lane that found g keeps its x and ys for the replay
             for (u64 i = 0; i < r; ++i) y = rho_step(R, y, c);
-            for (u64 k = 0; k < r && g == 1; k += 128) {
-                ys = y;
+            for (u64 k = 0; k < r && !stop; k += 128) {
+                if (g == 1) ys = y;
                 const u64 lim = min((u64)128, r - k);
                 for (u64 i = 0; i < lim; ++i) {
                     y = rho_step(R, y, c);
                     q = R.mul(q, x > y ? x - y : y - x);
                 }
-                g = gcd64(R.norm(q), n);
+                if (g == 1) g = gcd64(R.norm(q), n);
+                stop = __any_sync(FULL, g != 1 && g != n) || __all_sync(FULL, g != 1);
             }
-            r <<= 1;
         }
-        if (g == n) {
+        if (g == n) {                                  // replay this lane's last batch one step at a time
             g = 1;
-            for (u64 it = 0; it < (1ull << 26) && g == 1; ++it) {
+            for (u32 it = 0; it < 128 && g == 1; ++it) {
                 ys = rho_step(R, ys, c);
                 g = gcd64(x > ys ? x - ys : ys - x, n);
             }
         }
-        if (g != 1 && g != n) return g;
+        const u32 good = __ballot_sync(FULL, g != 1 && g != n);
+        if (good) return __shfl_sync(FULL, g, __ffs(good) - 1);
     }
     return 0;
 }
@@ -1933,9 +1938,7 @@ __device__ u64 warp_mult_order(u64 b, u64 p, const SieveTables& t, bool* failed)
                 if (!dup && nf < 24) f[nf++] = x;
                 continue;
             }
-            u64 dv = 0;
-            if (lane == 0) dv = rho_factor(x);
-            dv = __shfl_sync(FULL, dv, 0);
+            const u64 dv = warp_rho_factor(x);
             if (dv == 0 || sp + 2 > 8) {
                 *failed = true;
                 return 0;
@@ -1944,14 +1947,29 @@ __device__ u64 warp_mult_order(u64 b, u64 p, const SieveTables& t, bool* failed)
             stack[sp++] = x / dv;
         }
     }
+    // the order, one prime factor q of p - 1 per lane (nf <= 24): with q^k the
+    // power of q in p - 1, x = b^((p-1)/q^k) has order q^j, the q-part of
+    // ord_p(b); the order is the product of the lanes' parts
     Mont M;
     M.init(p);
     const u64 bm = M.to_mont(b % p, M.r2());
-    u64 order = pm1;
-    for (int i = 0; i < nf; ++i) {
-        while (order % f[i] == 0 && M.pow(bm, order / f[i]) == M.one) order /= f[i];
+    u64 q = 0;
+#pragma unroll
+    for (int i = 0; i < 24; ++i)
+        if (i < nf && (u32)i == lane) q = f[i];
+    u64 part = 1;
+    if (q) {
+        u64 t = pm1;
+        while (t % q == 0) t /= q;                     // t = (p - 1) / q^k
+        u64 x = M.pow(bm, t);
+        while (x != M.one) {
+            x = M.pow(x, q);
+            part *= q;
+        }
     }
-    return order;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) part *= __shfl_xor_sync(FULL, part, off);
+    return part;
 }
 
 // One warp per relation: exact primality of p (composite survivors are
