@@ -506,14 +506,21 @@ __device__ void bsgs_setup(const F& f, u64 p, u64 b_mod, u64 t, const DevItem& i
     if (jcount > p) jcount = p;                        // ord(B) < p (Math.hpp:398-400)
     const u64 L = it.cm * per;
     const u64 n_first = it.n_start + it.cm * k0;
-    const V bv = f.from_u64(b_mod);
-    const u64 G0 = f.residue(f.pow(bv, n_first));
+    // G0 = b^n_first and B = b^L from one chain of squarings of b
+    V sq = f.from_u64(b_mod), gv = f.one(), Bv = f.one();
+    for (u64 e1 = n_first, e2 = L; e1 | e2;) {
+        if (e1 & 1) gv = f.mul(gv, sq);
+        if (e2 & 1) Bv = f.mul(Bv, sq);
+        e1 >>= 1;
+        e2 >>= 1;
+        if (e1 | e2) sq = f.mul(sq, sq);
+    }
+    const u64 G0 = f.residue(gv);
     if (G0 == t) {                                     // j = 0
         emit_relation(p, n_first, 0, it.item_index, a.rel, a.rel_cap, ctr);
         return;
     }
     if (jcount <= 1) return;
-    const V Bv = f.pow(bv, L);
     u32 m = (u32)isqrt_ceil_dev(jcount);
     if (it.baby_scale != 256) m = max(1u, (u32)(((u64)m * it.baby_scale + 255) >> 8));
     // a whole number of baby iterations (lanes x chains per prime): the last

@@ -82,10 +82,10 @@ def test_bsgs_smallest_j(mps_lib, oracle, table_bits, table_kind):
 def test_order(siever, oracle):
     rng = random.Random(9)
     pairs = []
-    for p in oracle.primes(10**6, 10**6 + 3000) + oracle.primes(10**12, 10**12 + 3000) + \
-            [(1 << 61) - 1, 4_611_686_018_427_387_847, 1_111_111_111_111_111_111, 999_999_000_001] + \
-            # p - 1 = m q1 q2 with q1, q2 primes above 65521: the cofactor is split by the warp's rho
-            [32505883140163, 15332064649691, 41010969574327, 119026820723087, 664006356569749, 79226575236629]:
+    # the last six: p - 1 = m q1 q2 with q1, q2 primes above 65521, so the cofactor is split by rho
+    for p in (oracle.primes(10**6, 10**6 + 3000) + oracle.primes(10**12, 10**12 + 3000) +
+              [(1 << 61) - 1, 4_611_686_018_427_387_847, 1_111_111_111_111_111_111, 999_999_000_001] +
+              [32505883140163, 15332064649691, 41010969574327, 119026820723087, 664006356569749, 79226575236629]):
         pairs.append((rng.choice([2, 3, 5, 10, 12, 7]), p))
     want = [oracle.mult_order(b, p) for b, p in pairs]
     assert siever.order(pairs) == want
