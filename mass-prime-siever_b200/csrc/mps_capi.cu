@@ -396,6 +396,7 @@ int run_chunk(mps_ctx* c, u64 lo, u64 hi, u32 item, u64 K, const LaunchCfg& g_it
     pa.full_mr = c->tun.full_mr;
     pa.m_cap = launch_m_cap(c, g, tbits);
     pa.m_round = g.lanes * g.chains;
+    pa.prime_below = kSievedPrimeBelow;             // survivors of the sieve
 
     BsgsArgs ba{};
     ba.ent = c->d_ent;
@@ -562,6 +563,7 @@ int slot_enqueue(mps_ctx* c, WaveSlot& w, u32 tbits, const LaunchCfg& g, bool ca
     pa.full_mr = c->tun.full_mr;
     pa.m_cap = launch_m_cap(c, g, tbits);
     pa.m_round = g.lanes * g.chains;
+    pa.prime_below = kSievedPrimeBelow;             // survivors of the sieve
     BsgsArgs ba{};
     ba.ent = w.d_ent; ba.ent_cap = w.ent_cap; ba.rel = w.d_rel; ba.rel_cap = w.rel_cap; ba.tbits = tbits;
     ba.warps_per_block = warps; ba.persistent = 1; ba.chains = g.chains;

@@ -542,6 +542,7 @@ __device__ void bsgs_setup(const F& f, u64 p, u64 b_mod, u64 t, const DevItem& i
 
 template <class F>
 __device__ __forceinline__ bool stage1(u64 p, const PrepArgs& a) {
+    if (p < a.prime_below) return true;                // the sieve removed every composite below this
     F f;
     f.init(p);
     if (!sprp2_f(f, p)) return false;

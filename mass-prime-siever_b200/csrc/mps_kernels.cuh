@@ -85,7 +85,10 @@ struct PrepArgs {
     u32 full_mr;               // 1: 12-base Miller-Rabin on every survivor that passes the filters
     u32 m_cap;                 // baby steps per prime at most (what the launch's BSGS tables hold)
     u32 m_round;               // baby steps rounded up to a multiple of this (the BSGS iteration width)
+    u64 prime_below;           // survivors below this are prime (sieved by every prime up to their
+                               // square root: 65521^2 for the sieve's survivors, 0 for caller-given numbers)
 };
+constexpr u64 kSievedPrimeBelow = (u64)kSieveMaxPrime * kSieveMaxPrime;
 cudaError_t launch_prep(const PrepArgs& a, Counters* ctr, int grid, cudaStream_t s);
 
 // Exact BSGS, one warp per entry.

@@ -183,6 +183,7 @@ int run_pass(unsigned char* base, u64 lo, u64 hi, const DevItem& d, u32 tbits, i
     pa.rel_cap = kNoAllocRelations;
     pa.m_cap = std::min<u32>(noalloc_holds(tbits), kMaxBaby);
     pa.m_round = 64;                                         // one warp, two chains
+    pa.prime_below = kSievedPrimeBelow;                      // survivors of the sieve
     BsgsArgs ba{};
     ba.ent = ent;
     ba.ent_cap = kNoAllocEntries;
