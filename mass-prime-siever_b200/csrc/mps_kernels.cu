@@ -380,11 +380,17 @@ __device__ __forceinline__ bool prep_special(u64 p, const DevItem& it, const Pre
 // (t/p) = 1.  True when p can be dropped: a prime p then has no in-class
 // solution, and a composite p never gives a relation.  Costs two Jacobi
 // symbols of 32-bit numbers, before any modular exponentiation.
-__device__ __forceinline__ bool qr_reject(u64 p, const DevItem& it) {
+// The symbols themselves go to stage 2 in *quad (kQuadKnown | kQuadBNeg |
+// kQuadTNeg), where they stand for b^((p-1)/2) and t^((p-1)/2) (Euler).
+constexpr u32 kQuadKnown = 1u << 29, kQuadBNeg = 1u << 30, kQuadTNeg = 1u << 31;
+constexpr u32 kQuadBits = kQuadKnown | kQuadBNeg | kQuadTNeg;   // above every item index
+__device__ __forceinline__ bool qr_reject(u64 p, const DevItem& it, u32* quad) {
+    *quad = 0;
     if (!it.qr_on) return false;
     const int jb = jacobi_small(p, it.qr_neg[0], it.qr_k[0], it.qr_o[0], it.qr_rcp[0]);
     const int jt = jacobi_small(p, it.qr_neg[1], it.qr_k[1], it.qr_o[1], it.qr_rcp[1]);
     if (jb == 0 || jt == 0) return false;              // p shares a factor with b or c: the exact path decides
+    *quad = kQuadKnown | (jb < 0 ? kQuadBNeg : 0u) | (jt < 0 ? kQuadTNeg : 0u);
     if ((it.cm & 1) == 0) return (it.n_start & 1) ? jb != jt : jt != 1;
     return jb == 1 && jt != 1;
 }
@@ -409,19 +415,25 @@ __device__ __forceinline__ u32 gcd_Q(const DevItem& it, u64 pm1) {
 // residues of w and u in w_out, u_out for stage 2b).
 template <class F>
 __device__ __forceinline__ int power_split(const F& f, u64 p, u64 b_mod, u64 t, const DevItem& it, u32 walk, u32& d,
-                                           u32& r, u64& w_out, u64& u_out) {
+                                           u32& r, u64& w_out, u64& u_out, u32 quad) {
     typedef typename F::V V;
     const u64 pm1 = p - 1;
     const u32 g = gcd_Q(it, pm1);
-    const u64 e = exact_quotient(pm1, g);
-    V u = f.one(), w = f.one(), bu = f.from_u64(t), bw = f.from_u64(b_mod);
-    for (u64 x = e; x; x >>= 1) {                      // two exponentiations, interleaved
-        if (x & 1) {
-            u = f.mul(u, bu);
-            w = f.mul(w, bw);
+    V u = f.one(), w = f.one();
+    if (g == 2 && (quad & kQuadKnown)) {               // w, u = the prefilter's symbols (+-1)
+        if (quad & kQuadBNeg) w = f.from_u64(pm1);
+        if (quad & kQuadTNeg) u = f.from_u64(pm1);
+    } else {
+        const u64 e = exact_quotient(pm1, g);
+        V bu = f.from_u64(t), bw = f.from_u64(b_mod);
+        for (u64 x = e; x; x >>= 1) {                  // two exponentiations, interleaved
+            if (x & 1) {
+                u = f.mul(u, bu);
+                w = f.mul(w, bw);
+            }
+            bu = f.mul(bu, bu);
+            bw = f.mul(bw, bw);
         }
-        bu = f.mul(bu, bu);
-        bw = f.mul(bw, bw);
     }
     const V uc = f.canon(u), one = f.one();
     V x = one;
@@ -594,12 +606,12 @@ __device__ __forceinline__ void qpush(bool want, u32& n, u32* slot_out) {
 }
 
 template <class F>
-__device__ __forceinline__ int split_in(const DevItem& it, u64 p, u32& d, u32& r, u64& w, u64& u) {
+__device__ __forceinline__ int split_in(const DevItem& it, u64 p, u32& d, u32& r, u64& w, u64& u, u32 quad) {
     F f;
     f.init(p);
     const u64 bm = residue128(it.babs_hi, it.babs_lo, it.b_neg, p);
     const u64 t = p - residue128(it.cabs_hi, it.cabs_lo, it.c_neg, p);
-    return power_split(f, p, bm, t, it, kWalk, d, r, w, u);
+    return power_split(f, p, bm, t, it, kWalk, d, r, w, u, quad);
 }
 
 template <class F>
@@ -676,9 +688,11 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep(PrepArgs a, Counters* ctr
             if (lane < cnt) {
                 const u32 k = n1 - cnt + lane;
                 p = Q.p1[k];
-                item = Q.i1[k];
+                const u32 quad = Q.i1[k] & kQuadBits;
+                item = Q.i1[k] & ~kQuadBits;
                 const DevItem& it = a.items[item];
-                res = p < kFp64Limit ? split_in<FieldF>(it, p, d, r, w, u) : split_in<FieldM>(it, p, d, r, w, u);
+                res = p < kFp64Limit ? split_in<FieldF>(it, p, d, r, w, u, quad)
+                                     : split_in<FieldM>(it, p, d, r, w, u, quad);
             }
             n1 -= cnt;
             __syncwarp();
@@ -712,19 +726,19 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep(PrepArgs a, Counters* ctr
         const u64 k = first + lane;
         bool keep = false;
         u64 p = 0;
-        u32 item = a.item0;
+        u32 item = a.item0, quad = 0;
         if (k < n_surv) {
             p = a.surv[k];
             if (a.surv_item) item = a.surv_item[k];
             u64 bm, t;
-            if (prep_special(p, a.items[item], a, ctr, bm, t) && !qr_reject(p, a.items[item]))
+            if (prep_special(p, a.items[item], a, ctr, bm, t) && !qr_reject(p, a.items[item], &quad))
                 keep = p < kFp64Limit ? stage1<FieldF>(p, a) : stage1<FieldM>(p, a);
         }
         u32 s1;
         qpush(keep, n1, &s1);
         if (keep) {
             Q.p1[s1] = p;
-            Q.i1[s1] = item;
+            Q.i1[s1] = item | quad;                        // item indices stay below 2^29
         }
         __syncwarp();
     }
