@@ -380,10 +380,9 @@ __device__ __forceinline__ bool prep_special(u64 p, const DevItem& it, const Pre
 // (t/p) = 1.  True when p can be dropped: a prime p then has no in-class
 // solution, and a composite p never gives a relation.  Costs two Jacobi
 // symbols of 32-bit numbers, before any modular exponentiation.
-// The symbols themselves go to stage 2 in *quad (kQuadKnown | kQuadBNeg |
-// kQuadTNeg), where they stand for b^((p-1)/2) and t^((p-1)/2) (Euler).
-constexpr u32 kQuadKnown = 1u << 29, kQuadBNeg = 1u << 30, kQuadTNeg = 1u << 31;
-constexpr u32 kQuadBits = kQuadKnown | kQuadBNeg | kQuadTNeg;   // above every item index
+// The symbols themselves are returned in *quad (kQuadKnown | kQuadBNeg |
+// kQuadTNeg); for a prime p they are b^((p-1)/2) and t^((p-1)/2) (Euler).
+constexpr u32 kQuadKnown = 1u << 0, kQuadBNeg = 1u << 1, kQuadTNeg = 1u << 2;
 __device__ __forceinline__ bool qr_reject(u64 p, const DevItem& it, u32* quad) {
     *quad = 0;
     if (!it.qr_on) return false;
@@ -415,25 +414,20 @@ __device__ __forceinline__ u32 gcd_Q(const DevItem& it, u64 pm1) {
 // residues of w and u in w_out, u_out for stage 2b).
 template <class F>
 __device__ __forceinline__ int power_split(const F& f, u64 p, u64 b_mod, u64 t, const DevItem& it, u32 walk, u32& d,
-                                           u32& r, u64& w_out, u64& u_out, u32 quad) {
+                                           u32& r, u64& w_out, u64& u_out) {
     typedef typename F::V V;
     const u64 pm1 = p - 1;
     const u32 g = gcd_Q(it, pm1);
     V u = f.one(), w = f.one();
-    if (g == 2 && (quad & kQuadKnown)) {               // w, u = the prefilter's symbols (+-1)
-        if (quad & kQuadBNeg) w = f.from_u64(pm1);
-        if (quad & kQuadTNeg) u = f.from_u64(pm1);
-    } else {
-        const u64 e = exact_quotient(pm1, g);
-        V bu = f.from_u64(t), bw = f.from_u64(b_mod);
-        for (u64 x = e; x; x >>= 1) {                  // two exponentiations, interleaved
-            if (x & 1) {
-                u = f.mul(u, bu);
-                w = f.mul(w, bw);
-            }
-            bu = f.mul(bu, bu);
-            bw = f.mul(bw, bw);
+    const u64 e = exact_quotient(pm1, g);
+    V bu = f.from_u64(t), bw = f.from_u64(b_mod);
+    for (u64 x = e; x; x >>= 1) {                      // two exponentiations, interleaved
+        if (x & 1) {
+            u = f.mul(u, bu);
+            w = f.mul(w, bw);
         }
+        bu = f.mul(bu, bu);
+        bw = f.mul(bw, bw);
     }
     const V uc = f.canon(u), one = f.one();
     V x = one;
@@ -606,12 +600,23 @@ __device__ __forceinline__ void qpush(bool want, u32& n, u32* slot_out) {
 }
 
 template <class F>
-__device__ __forceinline__ int split_in(const DevItem& it, u64 p, u32& d, u32& r, u64& w, u64& u, u32 quad) {
+__device__ __forceinline__ int split_in(const DevItem& it, u64 p, u32& d, u32& r, u64& w, u64& u) {
     F f;
     f.init(p);
     const u64 bm = residue128(it.babs_hi, it.babs_lo, it.b_neg, p);
     const u64 t = p - residue128(it.cabs_hi, it.cabs_lo, it.c_neg, p);
-    return power_split(f, p, bm, t, it, kWalk, d, r, w, u, quad);
+    return power_split(f, p, bm, t, it, kWalk, d, r, w, u);
+}
+
+// The split of stage 2 without its exponentiations when g = gcd(Q, p - 1) = 2:
+// w = b^((p-1)/2) and u = t^((p-1)/2) are the prefilter's Jacobi symbols
+// (Euler).  w = 1: d = 1, and a solution needs u = 1; w = -1: d = 2, r = 0
+// for u = 1 and r = 1 for u = -1.  Returns false when there is no solution.
+__device__ __forceinline__ bool split_quadratic(u32 quad, u32& d, u32& r) {
+    const bool wneg = quad & kQuadBNeg, uneg = quad & kQuadTNeg;
+    d = wneg ? 2u : 1u;
+    r = uneg ? 1u : 0u;
+    return wneg || !uneg;
 }
 
 template <class F>
@@ -688,11 +693,9 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep(PrepArgs a, Counters* ctr
             if (lane < cnt) {
                 const u32 k = n1 - cnt + lane;
                 p = Q.p1[k];
-                const u32 quad = Q.i1[k] & kQuadBits;
-                item = Q.i1[k] & ~kQuadBits;
+                item = Q.i1[k];
                 const DevItem& it = a.items[item];
-                res = p < kFp64Limit ? split_in<FieldF>(it, p, d, r, w, u, quad)
-                                     : split_in<FieldM>(it, p, d, r, w, u, quad);
+                res = p < kFp64Limit ? split_in<FieldF>(it, p, d, r, w, u) : split_in<FieldM>(it, p, d, r, w, u);
             }
             n1 -= cnt;
             __syncwarp();
@@ -724,21 +727,34 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep(PrepArgs a, Counters* ctr
             continue;
         }
         const u64 k = first + lane;
-        bool keep = false;
+        bool keep = false, direct = false;
         u64 p = 0;
-        u32 item = a.item0, quad = 0;
+        u32 item = a.item0, quad = 0, d = 1, r = 0;
         if (k < n_surv) {
             p = a.surv[k];
             if (a.surv_item) item = a.surv_item[k];
             u64 bm, t;
-            if (prep_special(p, a.items[item], a, ctr, bm, t) && !qr_reject(p, a.items[item], &quad))
+            const DevItem& it = a.items[item];
+            if (prep_special(p, it, a, ctr, bm, t) && !qr_reject(p, it, &quad))
                 keep = p < kFp64Limit ? stage1<FieldF>(p, a) : stage1<FieldM>(p, a);
+            // g = 2 with the symbols known: the split is the symbols, straight to stage 3
+            if (keep && (quad & kQuadKnown) && gcd_Q(it, p - 1) == 2) {
+                direct = true;
+                keep = split_quadratic(quad, d, r);
+            }
         }
-        u32 s1;
-        qpush(keep, n1, &s1);
-        if (keep) {
+        // a queue holds fewer than 32 entries here (each is drained above at 32), so neither passes 63
+        u32 s1, s2;
+        qpush(keep && !direct, n1, &s1);
+        qpush(keep && direct, n2, &s2);
+        if (keep && !direct) {
             Q.p1[s1] = p;
-            Q.i1[s1] = item | quad;                        // item indices stay below 2^29
+            Q.i1[s1] = item;
+        } else if (keep) {
+            Q.p2[s2] = p;
+            Q.i2[s2] = item;
+            Q.d2[s2] = d;
+            Q.r2[s2] = r;
         }
         __syncwarp();
     }
