@@ -380,16 +380,11 @@ __device__ __forceinline__ bool prep_special(u64 p, const DevItem& it, const Pre
 // (t/p) = 1.  True when p can be dropped: a prime p then has no in-class
 // solution, and a composite p never gives a relation.  Costs two Jacobi
 // symbols of 32-bit numbers, before any modular exponentiation.
-// The symbols themselves are returned in *quad (kQuadKnown | kQuadBNeg |
-// kQuadTNeg); for a prime p they are b^((p-1)/2) and t^((p-1)/2) (Euler).
-constexpr u32 kQuadKnown = 1u << 0, kQuadBNeg = 1u << 1, kQuadTNeg = 1u << 2;
-__device__ __forceinline__ bool qr_reject(u64 p, const DevItem& it, u32* quad) {
-    *quad = 0;
+__device__ __forceinline__ bool qr_reject(u64 p, const DevItem& it) {
     if (!it.qr_on) return false;
     const int jb = jacobi_small(p, it.qr_neg[0], it.qr_k[0], it.qr_o[0], it.qr_rcp[0]);
     const int jt = jacobi_small(p, it.qr_neg[1], it.qr_k[1], it.qr_o[1], it.qr_rcp[1]);
     if (jb == 0 || jt == 0) return false;              // p shares a factor with b or c: the exact path decides
-    *quad = kQuadKnown | (jb < 0 ? kQuadBNeg : 0u) | (jt < 0 ? kQuadTNeg : 0u);
     if ((it.cm & 1) == 0) return (it.n_start & 1) ? jb != jt : jt != 1;
     return jb == 1 && jt != 1;
 }
@@ -418,9 +413,8 @@ __device__ __forceinline__ int power_split(const F& f, u64 p, u64 b_mod, u64 t, 
     typedef typename F::V V;
     const u64 pm1 = p - 1;
     const u32 g = gcd_Q(it, pm1);
-    V u = f.one(), w = f.one();
     const u64 e = exact_quotient(pm1, g);
-    V bu = f.from_u64(t), bw = f.from_u64(b_mod);
+    V u = f.one(), w = f.one(), bu = f.from_u64(t), bw = f.from_u64(b_mod);
     for (u64 x = e; x; x >>= 1) {                      // two exponentiations, interleaved
         if (x & 1) {
             u = f.mul(u, bu);
@@ -608,17 +602,6 @@ __device__ __forceinline__ int split_in(const DevItem& it, u64 p, u32& d, u32& r
     return power_split(f, p, bm, t, it, kWalk, d, r, w, u);
 }
 
-// The split of stage 2 without its exponentiations when g = gcd(Q, p - 1) = 2:
-// w = b^((p-1)/2) and u = t^((p-1)/2) are the prefilter's Jacobi symbols
-// (Euler).  w = 1: d = 1, and a solution needs u = 1; w = -1: d = 2, r = 0
-// for u = 1 and r = 1 for u = -1.  Returns false when there is no solution.
-__device__ __forceinline__ bool split_quadratic(u32 quad, u32& d, u32& r) {
-    const bool wneg = quad & kQuadBNeg, uneg = quad & kQuadTNeg;
-    d = wneg ? 2u : 1u;
-    r = uneg ? 1u : 0u;
-    return wneg || !uneg;
-}
-
 template <class F>
 __device__ __forceinline__ bool split_pp_in(const DevItem& it, u64 p, u64 w, u64 u, u32& d, u32& r) {
     F f;
@@ -727,34 +710,21 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep(PrepArgs a, Counters* ctr
             continue;
         }
         const u64 k = first + lane;
-        bool keep = false, direct = false;
+        bool keep = false;
         u64 p = 0;
-        u32 item = a.item0, quad = 0, d = 1, r = 0;
+        u32 item = a.item0;
         if (k < n_surv) {
             p = a.surv[k];
             if (a.surv_item) item = a.surv_item[k];
             u64 bm, t;
-            const DevItem& it = a.items[item];
-            if (prep_special(p, it, a, ctr, bm, t) && !qr_reject(p, it, &quad))
+            if (prep_special(p, a.items[item], a, ctr, bm, t) && !qr_reject(p, a.items[item]))
                 keep = p < kFp64Limit ? stage1<FieldF>(p, a) : stage1<FieldM>(p, a);
-            // g = 2 with the symbols known: the split is the symbols, straight to stage 3
-            if (keep && (quad & kQuadKnown) && gcd_Q(it, p - 1) == 2) {
-                direct = true;
-                keep = split_quadratic(quad, d, r);
-            }
         }
-        // a queue holds fewer than 32 entries here (each is drained above at 32), so neither passes 63
-        u32 s1, s2;
-        qpush(keep && !direct, n1, &s1);
-        qpush(keep && direct, n2, &s2);
-        if (keep && !direct) {
+        u32 s1;
+        qpush(keep, n1, &s1);
+        if (keep) {
             Q.p1[s1] = p;
             Q.i1[s1] = item;
-        } else if (keep) {
-            Q.p2[s2] = p;
-            Q.i2[s2] = item;
-            Q.d2[s2] = d;
-            Q.r2[s2] = r;
         }
         __syncwarp();
     }
