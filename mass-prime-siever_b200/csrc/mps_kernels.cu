@@ -402,36 +402,11 @@ __device__ __forceinline__ u32 gcd_Q(const DevItem& it, u64 pm1) {
     return gcd32(it.Q, rem);
 }
 
-// The walk of the split: d = ord(w) and r with w^r == u, for w, u in the
-// g-th roots of unity, by at most `walk` steps.  Returns 0 (no r: no
-// solution), 1 (d, r found) or 2 (d > walk: not decided).
-template <class F>
-__device__ __forceinline__ int walk_split(const F& f, typename F::V w, typename F::V u, u32 g, u32 walk, u32& d,
-                                          u32& r) {
-    typedef typename F::V V;
-    const V uc = f.canon(u), one = f.one();
-    V x = one;
-    bool found = false;
-    const u32 lim = min(g, walk);
-    for (u32 k = 0; k < lim; ++k) {                    // discrete log in <w>
-        if (!found && f.eq(x, uc)) {
-            r = k;
-            found = true;
-        }
-        x = f.mul(x, w);
-        if (f.eq(x, one)) {
-            d = k + 1;
-            return found ? 1 : 0;
-        }
-    }
-    return lim == g ? 0 : 2;
-}
-
 // Stage 2: with g = gcd(Q, p - 1) and e = (p - 1) / g, w = b^e and u = t^e
 // are g-th roots of unity and b^n == t forces w^n == u, i.e. n == r (mod d),
 // d = ord(w) -- or there is no solution.  Returns 0 (no solution), 1 (d, r
 // found by a walk of at most `walk` steps) or 2 (longer: deferred, with the
-// residues of w and u in w_out, u_out for the longer walk and stage 2b).
+// residues of w and u in w_out, u_out for stage 2b).
 template <class F>
 __device__ __forceinline__ int power_split(const F& f, u64 p, u64 b_mod, u64 t, const DevItem& it, u32 walk, u32& d,
                                            u32& r, u64& w_out, u64& u_out) {
@@ -448,12 +423,25 @@ __device__ __forceinline__ int power_split(const F& f, u64 p, u64 b_mod, u64 t, 
         bu = f.mul(bu, bu);
         bw = f.mul(bw, bw);
     }
-    const int res = walk_split(f, w, u, g, walk, d, r);
-    if (res == 2) {
-        w_out = f.residue(w);
-        u_out = f.residue(u);
+    const V uc = f.canon(u), one = f.one();
+    V x = one;
+    bool found = false;
+    const u32 lim = min(g, walk);
+    for (u32 k = 0; k < lim; ++k) {                    // discrete log in <w>
+        if (!found && f.eq(x, uc)) {
+            r = k;
+            found = true;
+        }
+        x = f.mul(x, w);
+        if (f.eq(x, one)) {
+            d = k + 1;
+            return found ? 1 : 0;
+        }
     }
-    return res;
+    if (lim == g) return 0;
+    w_out = f.residue(w);
+    u_out = f.residue(u);
+    return 2;
 }
 
 // Stage 2b: the same split for long orders, one prime power of g at a time,
@@ -562,12 +550,7 @@ __device__ __forceinline__ bool stage1(u64 p, const PrepArgs& a) {
 }
 
 constexpr u32 kPrepThreads = 256;
-// Stage 2 walks at most kWalk steps; primes left undecided walk again, up to
-// kWalkLong steps, in warps of their own (stage 2w), and only those left then
-// go to stage 2b.  A warp walks as long as its slowest lane, so the primes
-// with short orders (most of them) are not held up by the others.
-constexpr u32 kWalk = 16;
-constexpr u32 kWalkLong = 48;
+constexpr u32 kWalk = 48;                              // stage-2 walk before deferring
 
 // Warp-aggregated push onto a shared-memory queue.
 __device__ __forceinline__ u32 queue_slot(u32* count, bool want) {
@@ -583,11 +566,9 @@ __device__ __forceinline__ u32 queue_slot(u32* count, bool want) {
 
 // The prep: one persistent kernel without block barriers.  Every warp claims
 // 32 survivors at a time and carries them through the stages on its own,
-// with four warp-private queues in shared memory between the stages
+// with three warp-private queues in shared memory between the stages
 // (survivors that passed stage 1; primes with their (d, r) for stage 3;
-// primes for the longer walk of stage 2w; primes deferred to stage 2b).  The
-// later stages drain first, so when a stage runs, every queue it pushes into
-// holds fewer than 32 entries.  A queue is drained whenever it holds 32
+// primes deferred to stage 2b).  A queue is drained whenever it holds 32
 // entries, so every stage runs with full warps, and a warp never waits for
 // another; the partial queues are drained at the end.  A queue never holds
 // more than 63 entries: a stage pushes at most 32 into a queue that held
@@ -602,8 +583,6 @@ struct PrepQueues {
     u64 pd[64];
     u64 wd[64], ud[64];                            // stage 2's w and u of a deferred prime
     u32 id[64];
-    u64 pw[64], ww[64], uw[64];                    // primes for the longer walk, with stage 2's w and u
-    u32 iw[64];
 };
 
 // Appends the lanes with want to a warp queue of n entries (n warp-uniform).
@@ -621,15 +600,6 @@ __device__ __forceinline__ int split_in(const DevItem& it, u64 p, u32& d, u32& r
     const u64 bm = residue128(it.babs_hi, it.babs_lo, it.b_neg, p);
     const u64 t = p - residue128(it.cabs_hi, it.cabs_lo, it.c_neg, p);
     return power_split(f, p, bm, t, it, kWalk, d, r, w, u);
-}
-
-// Stage 2w: the longer walk for a prime whose short walk did not decide it,
-// from stage 2's w and u (residues).
-template <class F>
-__device__ __forceinline__ int walk_in(const DevItem& it, u64 p, u64 w, u64 u, u32 walk, u32& d, u32& r) {
-    F f;
-    f.init(p);
-    return walk_split(f, f.from_u64(w), f.from_u64(u), gcd_Q(it, p - 1), walk, d, r);
 }
 
 template <class F>
@@ -653,10 +623,10 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep(PrepArgs a, Counters* ctr
     PrepQueues& Q = qs[threadIdx.x >> 5];
     const u32 lane = threadIdx.x & 31;
     const u64 n_surv = min((u64)*(volatile unsigned long long*)&ctr->survivors, a.surv_cap);
-    u32 n1 = 0, n2 = 0, nd = 0, nw = 0;                  // queue lengths (warp-uniform)
+    u32 n1 = 0, n2 = 0, nd = 0;                          // queue lengths (warp-uniform)
     bool inputs = true;
     for (;;) {
-        if (n2 >= 32 || (!inputs && n1 == 0 && nw == 0 && nd == 0 && n2 > 0)) {
+        if (n2 >= 32 || (!inputs && n1 == 0 && nd == 0 && n2 > 0)) {
             // stage 3: class combination and the BSGS set-up
             const u32 cnt = min(n2, 32u);
             if (lane < cnt) {
@@ -670,7 +640,7 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep(PrepArgs a, Counters* ctr
             __syncwarp();
             continue;
         }
-        if (nd >= 32 || (!inputs && n1 == 0 && nw == 0 && nd > 0)) {
+        if (nd >= 32 || (!inputs && n1 == 0 && nd > 0)) {
             // stage 2b: long orders, one prime power at a time
             const u32 cnt = min(nd, 32u);
             bool ok = false;
@@ -697,41 +667,6 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep(PrepArgs a, Counters* ctr
             __syncwarp();
             continue;
         }
-        if (nw >= 32 || (!inputs && n1 == 0 && nw > 0)) {
-            // stage 2w: the longer walk, then stage 2b for what is left
-            const u32 cnt = min(nw, 32u);
-            int res = 0;
-            u32 d = 1, r = 0, item = 0;
-            u64 p = 0, w = 0, u = 0;
-            if (lane < cnt) {
-                const u32 k = nw - cnt + lane;
-                p = Q.pw[k];
-                w = Q.ww[k];
-                u = Q.uw[k];
-                item = Q.iw[k];
-                const DevItem& it = a.items[item];
-                res = p < kFp64Limit ? walk_in<FieldF>(it, p, w, u, kWalkLong, d, r)
-                                     : walk_in<FieldM>(it, p, w, u, kWalkLong, d, r);
-            }
-            nw -= cnt;
-            __syncwarp();
-            u32 s2, sd;
-            qpush(res == 1, n2, &s2);
-            qpush(res == 2, nd, &sd);
-            if (res == 1) {
-                Q.p2[s2] = p;
-                Q.i2[s2] = item;
-                Q.d2[s2] = d;
-                Q.r2[s2] = r;
-            } else if (res == 2) {
-                Q.pd[sd] = p;
-                Q.wd[sd] = w;
-                Q.ud[sd] = u;
-                Q.id[sd] = item;
-            }
-            __syncwarp();
-            continue;
-        }
         if (n1 >= 32 || (!inputs && n1 > 0)) {
             // stage 2: power-residue split with a short walk
             const u32 cnt = min(n1, 32u);
@@ -747,19 +682,19 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep(PrepArgs a, Counters* ctr
             }
             n1 -= cnt;
             __syncwarp();
-            u32 s2, sw;
+            u32 s2, sd;
             qpush(res == 1, n2, &s2);
-            qpush(res == 2, nw, &sw);
+            qpush(res == 2, nd, &sd);
             if (res == 1) {
                 Q.p2[s2] = p;
                 Q.i2[s2] = item;
                 Q.d2[s2] = d;
                 Q.r2[s2] = r;
             } else if (res == 2) {
-                Q.pw[sw] = p;
-                Q.ww[sw] = w;
-                Q.uw[sw] = u;
-                Q.iw[sw] = item;
+                Q.pd[sd] = p;
+                Q.wd[sd] = w;
+                Q.ud[sd] = u;
+                Q.id[sd] = item;
             }
             __syncwarp();
             continue;
