@@ -123,3 +123,12 @@ def test_counts_consistent(oracle):
     assert 0 < cnt["bsgs_primes"] < cnt["primes"]
     m = math.isqrt(10**7 // 6) + 1
     assert cnt["bsgs_mmul"] <= cnt["bsgs_primes"] * 2 * (m + 2)
+
+
+def test_mult_order_when_p_minus_1_has_two_large_factors(oracle):
+    """p - 1 = m q1 q2 with q1, q2 primes above 65521: the order needs the
+    cofactor split (rho on the device).  The oracle's order is the true order."""
+    sympy = pytest.importorskip("sympy")
+    for p in (32505883140163, 15332064649691, 41010969574327, 119026820723087, 664006356569749, 79226575236629):
+        for b in (2, 3, 10, 12):
+            assert oracle.mult_order(b, p) == sympy.n_order(b, p), (b, p)
